@@ -1,0 +1,182 @@
+/*
+ * tasep.h - C ABI of the B200 TASEP master-equation integrator
+ *           (libtasep_cuda.so, sm_100a).
+ *
+ * The reference (KilianPiochUBT/TASEP) has no plugin or FFI layer: its hot
+ * path is the step loop of bin/masterEquation calling the C functions of
+ * src/lib/solv.c and src/lib/matgen.c.  Each entry point below names the
+ * reference code it replaces.  Plain C types only; no CUDA or torch types in
+ * any signature (streams are passed as void*, i.e. a cudaStream_t).
+ *
+ * State convention (as in the reference): N = 2^n states, bit b of a state
+ * index is lattice site n-1-b (site 0 = entry site).  Rates r[0..n]:
+ * r[0] = alpha (entry into site 0), r[j] = hop rate site j-1 -> j
+ * (j = 1..n-1), r[n] = beta (exit from site n-1)
+ * (reference src/masterEquation.c:457-460, src/lib/matgen.c:29-67).
+ *
+ * Errors: every call returns a tasep_status; tasep_last_error() gives a
+ * thread-local message.  Nothing prints and nothing calls exit() (the
+ * reference exits with -1 through err_exit, src/lib/io.c:13-19).
+ */
+#ifndef TASEP_H
+#define TASEP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TASEP_ABI_VERSION 1
+#define TASEP_MAX_N 33
+
+typedef enum {
+    TASEP_OK = 0,
+    TASEP_ERR_INVALID = 1,     /* bad argument or call order */
+    TASEP_ERR_NOMEM = 2,       /* device allocation failed */
+    TASEP_ERR_CUDA = 3,        /* CUDA runtime error */
+    TASEP_ERR_NODEV = 4,       /* no usable CUDA device */
+    TASEP_ERR_TIMEOUT = 5,     /* a bounded device-side wait expired */
+    TASEP_ERR_UNSUPPORTED = 6  /* combination not implemented */
+} tasep_status;
+
+/* Integrators.
+ * REF: the reference's step, bit for bit.  Its four stage calls all gather
+ *      from the state (src/masterEquation.c:630-636, src/lib/solv.c:13), so a
+ *      step is x += (k+2k+2k+k)/6 with k = h*M*x (one generator application).
+ * RK4: classical fourth-order Runge-Kutta (four generator applications). */
+enum { TASEP_INTEGRATOR_REF = 0, TASEP_INTEGRATOR_RK4 = 1 };
+
+/* FP64: every vector in double.  MIXED (RK4 with constant rates only): the
+ * state, the convergence norm and the final update stay in double; the three
+ * stage vectors and their generator gathers are float. */
+enum { TASEP_PRECISION_FP64 = 0, TASEP_PRECISION_MIXED = 1 };
+
+/* Initial states: UNIFORM = 2^-n everywhere (src/masterEquation.c:402-409),
+ * EMPTY = empty lattice, P(state 0) = 1. */
+enum { TASEP_INIT_UNIFORM = 0, TASEP_INIT_EMPTY = 1 };
+
+/* Time-variant rate functions (src/lib/matvec.c:44-68):
+ * SIN: A*sin(w*t+phi)+c, COS: A*cos(w*t+phi)+c, LIN: A*t+c; clamped at 0. */
+enum { TASEP_FUN_SIN = 0, TASEP_FUN_COS = 1, TASEP_FUN_LIN = 2 };
+
+typedef struct tasep_meq tasep_meq; /* opaque; owns all device buffers */
+
+typedef struct {
+    int n;          /* lattice length, 1..TASEP_MAX_N */
+    int integrator; /* TASEP_INTEGRATOR_* */
+    int precision;  /* TASEP_PRECISION_* */
+    int device;     /* CUDA device ordinal; -1 = the current device */
+    void *stream;   /* cudaStream_t to launch on; NULL = the handle makes one */
+} tasep_meq_config;
+
+typedef struct {
+    double t0;       /* start time; time-variant rates are evaluated from it */
+    double h;        /* step size, h = (T - t)/steps in the reference (:586) */
+    uint64_t steps;  /* maximum number of steps (-s) */
+    double stop_tol; /* exit test: L1 norm of the increment < stop_tol*h ...  */
+    int stop_count;  /* ... on more than stop_count consecutive steps          */
+    int exit_rule;   /* 1 = apply the rule (src/masterEquation.c:670-679);
+                        0 = run every step (the reference time-var loop) */
+} tasep_run_config;
+
+typedef struct {
+    uint64_t steps_done;    /* loop iterations executed */
+    uint64_t steps_at_stop; /* index of the last qualifying step */
+    int early_stop;         /* qualifying steps in a row at the end */
+    int converged;          /* 1 if the loop ended through the exit rule */
+    double last_checksum;   /* L1 norm of the last increment */
+    double t_end;           /* t0 + h added steps_done times */
+} tasep_run_result;
+
+/* ---- handle lifecycle --------------------------------------------------
+ * Replaces the allocations of src/masterEquation.c:354-505 (x, x1, k1..k4)
+ * and, for -f, :586-616 (the CSR arrays): the generator is never stored. */
+tasep_status tasep_meq_create(const tasep_meq_config *cfg, tasep_meq **out);
+tasep_status tasep_meq_destroy(tasep_meq *m);
+
+/* Rates r[0..n] (n+1 doubles).  Replaces the -i file / --alpha --beta
+ * --gamma set-up of src/masterEquation.c:432-461. */
+tasep_status tasep_meq_set_rates(tasep_meq *m, const double *rates);
+
+/* Time-variant rates, n+1 entries each; evaluated on the device at every
+ * stage time.  Replaces the per-step timeVariantProbs call
+ * (src/masterEquation.c:886, src/lib/matvec.c:44-68).  REF evaluates all
+ * of a step at its start time t, as the reference does; RK4 at t, t+h/2,
+ * t+h/2, t+h. */
+tasep_status tasep_meq_set_timevar(tasep_meq *m, const int *type, const double *amplitude,
+                                   const double *period, const double *offset,
+                                   const double *constant);
+tasep_status tasep_meq_clear_timevar(tasep_meq *m);
+
+/* Initial state.  Replaces src/masterEquation.c:402-409. */
+tasep_status tasep_meq_init(tasep_meq *m, int kind);
+/* Initial state from a host vector of 2^n doubles. */
+tasep_status tasep_meq_load(tasep_meq *m, const double *host_x);
+
+/* The integration loop with its exit rule.  Replaces the step loops of
+ * src/masterEquation.c:628-682 (-f), :883-921 (time-var) and :929-982 (per
+ * row), including rk4_step / rk4_step_reduced / gen_meq_row
+ * (src/lib/solv.c:3-135).  Blocks until the loop ends. */
+tasep_status tasep_meq_run(tasep_meq *m, const tasep_run_config *rc, tasep_run_result *res);
+
+/* Enqueues `steps` steps on the handle's stream without the exit rule and
+ * without waiting (benchmarks, CUDA-graph capture); t advances by h. */
+tasep_status tasep_meq_enqueue_steps(tasep_meq *m, double t0, double h, uint64_t steps);
+tasep_status tasep_meq_synchronize(tasep_meq *m);
+
+/* Copies probabilities [offset, offset+count) of the state to host memory. */
+tasep_status tasep_meq_store(const tasep_meq *m, double *host_x, uint64_t offset, uint64_t count);
+
+/* Observables of the current state, each output optional (NULL skips it):
+ *   rho[b]   - per-bit densities, bit order (condense / exp_val_eval,
+ *              src/lib/matvec.c:10-42, :70-91); site j is rho[n-1-j];
+ *   cov      - n*n covariance in site order, as src/masterEquation.c:1121-1139;
+ *   mul      - n*n y_k*y_i + cov, as src/masterEquation.c:1289-1302;
+ *   window4  - (n-3)*16 marginals of the 4-bit windows: window4[p*16+q] =
+ *              sum over states whose bits p..p+3 equal q (feeds the window
+ *              observables of src/masterEquation.c:32-143, :1422-1539);
+ *   mass     - sum of all probabilities. */
+tasep_status tasep_meq_observables(tasep_meq *m, double *rho, double *cov, double *mul,
+                                   double *window4, double *mass);
+
+/* cudaStream_t the handle launches on. */
+void *tasep_meq_stream(const tasep_meq *m);
+
+/* Per-kernel device time (CUDA events around each launch on the handle's
+ * stream).  enable=1 starts recording and clears the totals. */
+tasep_status tasep_meq_profile(tasep_meq *m, int enable);
+/* names[i] (static strings), total milliseconds and launch counts of up to
+ * `cap` kernels; returns the number of kernels in *count. */
+tasep_status tasep_meq_profile_read(tasep_meq *m, const char **names, double *ms,
+                                    uint64_t *launches, int cap, int *count);
+
+/* ---- device-pointer operators ------------------------------------------
+ * For callers that keep their own device vectors.  x, y: 2^n doubles in
+ * device memory; rates: n+1 doubles in host memory; stream may be NULL. */
+
+/* y = M x, each row summed in the reference's entry order (entry, diagonal,
+ * exit, hops by ascending bit) with separate multiply and add, so y equals
+ * the CSR product of gencrs + rk4_step's gather bit for bit
+ * (src/lib/matgen.c:7-74, src/lib/solv.c:9-13). */
+tasep_status tasep_apply_device(int n, const double *rates, const double *x, double *y,
+                                void *stream);
+
+/* One reference step x_out = x + (k+2k+2k+k)/6, k = h*M*x, and its L1 norm
+ * written to *checksum_host (src/masterEquation.c:628-642).  x and x_out must
+ * not overlap.  Scratch for the norm is allocated on the first call per
+ * device and reused. */
+tasep_status tasep_step_ref_device(int n, const double *rates, double h, const double *x,
+                                   double *x_out, double *checksum_host, void *stream);
+
+/* ---- misc ---------------------------------------------------------------- */
+const char *tasep_last_error(void);
+int tasep_abi_version(void);
+/* Bytes of device memory a handle with this configuration allocates. */
+uint64_t tasep_meq_footprint(int n, int integrator, int precision, int timevar);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

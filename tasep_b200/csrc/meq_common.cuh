@@ -1,0 +1,211 @@
+// meq_common.cuh - shared types and sm_100a PTX helpers for the TASEP
+// master-equation kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tasep {
+
+constexpr int kMaxN = 33;
+constexpr int kMaxR = kMaxN + 1;
+
+// Kernel flavours.  REF is the reference step; H1..H4 the four stages of
+// classical RK4 written as a Horner scheme (constant rates); U1..U4 the four
+// stages of classical RK4 with materialised stage inputs (time-variant
+// rates); APPLY is y = M x.
+enum Stage : int {
+    ST_REF = 0, ST_H1, ST_H2, ST_H3, ST_H4, ST_U1, ST_U2, ST_U3, ST_U4, ST_APPLY, ST_COUNT
+};
+
+// Exit-rule state kept on the device so that steps can be enqueued ahead of
+// the host (src/masterEquation.c:670-679).
+struct ExitState {
+    int done;
+    int converged;
+    int early_stop;
+    int error;  // 0 ok, 1 = a bounded wait expired
+    unsigned long long steps_at_stop;
+    unsigned long long steps_done;
+    double last_checksum;
+    double pad;
+};
+
+// Rates for one launch: constant, or the time-variant functions of
+// src/lib/matvec.c:44-68 evaluated at the stage time.
+struct RateSpec {
+    double r[kMaxR];
+    double amp[kMaxR], per[kMaxR], off[kMaxR], cst[kMaxR];
+    int type[kMaxR];
+    int timevar;
+};
+
+// One rate at time t, with the reference's separate roundings
+// (amplitude*sin(t*period + offset) + constant, clamped at 0).
+__device__ __forceinline__ double rate_at(const RateSpec &rs, int i, double t) {
+    if (!rs.timevar) return rs.r[i];
+    double v;
+    switch (rs.type[i]) {
+    case 0: v = __dadd_rn(__dmul_rn(rs.amp[i], sin(__dadd_rn(__dmul_rn(t, rs.per[i]), rs.off[i]))), rs.cst[i]); break;
+    case 1: v = __dadd_rn(__dmul_rn(rs.amp[i], cos(__dadd_rn(__dmul_rn(t, rs.per[i]), rs.off[i]))), rs.cst[i]); break;
+    case 2: v = __dadd_rn(__dmul_rn(rs.amp[i], t), rs.cst[i]); break;
+    default: return rs.r[i];
+    }
+    return v < 0.0 ? 0.0 : v;
+}
+
+// Arithmetic with or without contraction.  EXACT keeps every multiply and add
+// separately rounded, as the reference's C (ISO mode, no contraction).
+template <typename T, bool EXACT> struct Ar;
+template <> struct Ar<double, true> {
+    static __device__ __forceinline__ double madd(double acc, double a, double b) { return __dadd_rn(acc, __dmul_rn(a, b)); }
+    static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+};
+template <> struct Ar<double, false> {
+    static __device__ __forceinline__ double madd(double acc, double a, double b) { return fma(a, b, acc); }
+    static __device__ __forceinline__ double sub(double a, double b) { return a - b; }
+};
+template <> struct Ar<float, true> {
+    static __device__ __forceinline__ float madd(float acc, float a, float b) { return __fadd_rn(acc, __fmul_rn(a, b)); }
+    static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+};
+template <> struct Ar<float, false> {
+    static __device__ __forceinline__ float madd(float acc, float a, float b) { return fmaf(a, b, acc); }
+    static __device__ __forceinline__ float sub(float a, float b) { return a - b; }
+};
+
+// ---- PTX helpers (mbarrier, bulk async copies, cache policies) ----------
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_timer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: gives up after ~2 s (or as soon as another thread has
+// flagged an error), records the error and returns false.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *err_flag) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_timer_ns();
+    for (uint32_t it = 0;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 63) == 63) {
+            if (*err_flag) return false;
+            if (global_timer_ns() - t0 > kWaitLimitNs) {
+                *err_flag = 1;
+                return false;
+            }
+        }
+    }
+}
+
+// Bounded wait that ignores the error flag: used on the error path to let
+// copies already issued land before the CTA exits.
+__device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
+    const uint64_t t0 = global_timer_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (global_timer_ns() - t0 > limit_ns) return;
+}
+
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// Bulk global -> shared copy completing on an mbarrier (no multicast).
+// dst, src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                         uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+// 4-element vector load from shared memory.
+template <typename T> struct V4;
+template <> struct V4<double> {
+    static __device__ __forceinline__ void lds(const double *p, double &a, double &b, double &c, double &d) {
+        const double2 u = reinterpret_cast<const double2 *>(p)[0];
+        const double2 v = reinterpret_cast<const double2 *>(p)[1];
+        a = u.x; b = u.y; c = v.x; d = v.y;
+    }
+    static __device__ __forceinline__ void lds2(const double *p, double &a, double &b) {
+        const double2 u = reinterpret_cast<const double2 *>(p)[0];
+        a = u.x; b = u.y;
+    }
+    static __device__ __forceinline__ void stg(double *p, double a, double b, double c, double d, uint64_t pol) {
+        asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(a), "d"(b),
+                     "l"(pol)
+                     : "memory");
+        asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p + 2), "d"(c),
+                     "d"(d), "l"(pol)
+                     : "memory");
+    }
+};
+template <> struct V4<float> {
+    static __device__ __forceinline__ void lds(const float *p, float &a, float &b, float &c, float &d) {
+        const float4 u = reinterpret_cast<const float4 *>(p)[0];
+        a = u.x; b = u.y; c = u.z; d = u.w;
+    }
+    static __device__ __forceinline__ void lds2(const float *p, float &a, float &b) {
+        const float2 u = reinterpret_cast<const float2 *>(p)[0];
+        a = u.x; b = u.y;
+    }
+    static __device__ __forceinline__ void stg(float *p, float a, float b, float c, float d, uint64_t pol) {
+        asm volatile("st.global.L1::no_allocate.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(a),
+                     "f"(b), "f"(c), "f"(d), "l"(pol)
+                     : "memory");
+    }
+};
+
+// Deterministic warp sum (fixed xor tree).
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+}  // namespace tasep

@@ -1,0 +1,469 @@
+// meq_tile.cuh - matrix-free generator sweep for n > kTileBits.
+//
+// One launch applies the TASEP generator M once to a "gathered" vector g and
+// fuses the stage's epilogue (axpy, RK4 combination, L1 norm of the
+// increment, exit rule).  M is never stored: each state i gathers its
+// in-flows (entry, diagonal, exit, hops) from bit-flipped neighbours, in the
+// reference's row order (src/lib/solv.c:81-135; src/lib/matgen.c:29-67):
+//   1. entry from i - 2^(n-1) if bit n-1 of i is set, rate r[0];
+//   2. diagonal -(r[n][b0] + r[0][!b(n-1)] + sum_j r[n-1-j][!b_j & b_(j+1)]),
+//      subtracted in that order;
+//   3. exit from i+1 if bit 0 is clear, rate r[n];
+//   4. hops from i + 2^k for k ascending where b_k & !b_(k+1), rate r[n-1-k].
+//
+// Layout: the state vector is one flat array in reference index order.  A
+// tile is 2^kTileBits consecutive states; tile T's high bits are the state's
+// bits >= kTileBits.  Per CTA (one per SM, persistent):
+//   * a producer warp streams, with cp.async.bulk (no multicast), the tile of
+//     g and of each per-state extra input into a double-buffered stage, then
+//     every partner tile this tile needs - the entry tile, the lower half of
+//     tile T+1 (the hop straddling the tile boundary) and one tile per active
+//     high hop - into a ring of shared-memory slots;
+//   * 8 consumer warps own 4 consecutive states per group, 2 groups each.
+//     Hops inside a group are register moves, hops between groups read the
+//     staged tile, high hops read the ring slots in ascending bit order, so
+//     the reference's summation order is kept exactly.
+// Tiles are visited in natural order by all CTAs together, so partner tiles
+// up to a few tens of MB ahead are still in L2 when they are gathered.
+#pragma once
+
+#include "meq_common.cuh"
+
+namespace tasep {
+
+constexpr int kTileBits = 11;
+constexpr int kTile = 1 << kTileBits;               // states per tile
+constexpr int kConsumerWarps = 8;
+constexpr int kConsumers = kConsumerWarps * 32;      // 256
+constexpr int kTileThreads = kConsumers + 32;        // + producer warp
+constexpr int kRingSlots = 4;
+static_assert(kTile / 4 == 2 * kConsumers, "two groups of four states per consumer thread");
+
+struct TileParams {
+    int n;
+    unsigned long long ntiles;
+    const void *g;             // gathered vector
+    const void *s0, *s1, *s2;  // per-state extra inputs
+    void *out;
+    double h, hc;              // step and stage coefficient
+    double t;                  // stage time
+    double *partials;          // per-CTA L1 partial sums (final stages)
+    unsigned int *counter;     // last-CTA ticket
+    ExitState *ex;
+    unsigned long long step;   // step index (exit rule)
+    double thresh;             // stop_tol * h
+    int stop_count;
+    int exit_rule;
+    int skip_if_done;
+    RateSpec rs;
+};
+
+// Per-stage types: G gathered, O output, X0..X2 extras (NX used).
+template <int S, typename E> struct StageT;
+template <typename E> struct StageT<ST_APPLY, E> {
+    using G = double; using O = double; using X0 = double; using X1 = double; using X2 = double;
+    static constexpr int NX = 0; static constexpr bool FINAL = false; static constexpr bool EXACT = true;
+};
+template <typename E> struct StageT<ST_REF, E> {
+    using G = double; using O = double; using X0 = double; using X1 = double; using X2 = double;
+    static constexpr int NX = 0; static constexpr bool FINAL = true; static constexpr bool EXACT = true;
+};
+template <typename E> struct StageT<ST_H1, E> {
+    using G = double; using O = E; using X0 = double; using X1 = double; using X2 = double;
+    static constexpr int NX = 0; static constexpr bool FINAL = false; static constexpr bool EXACT = false;
+};
+template <typename E> struct StageT<ST_H2, E> {
+    using G = E; using O = E; using X0 = E; using X1 = E; using X2 = E;
+    static constexpr int NX = 0; static constexpr bool FINAL = false; static constexpr bool EXACT = false;
+};
+template <typename E> struct StageT<ST_H3, E> {
+    using G = E; using O = E; using X0 = E; using X1 = E; using X2 = E;
+    static constexpr int NX = 1; static constexpr bool FINAL = false; static constexpr bool EXACT = false;
+};
+template <typename E> struct StageT<ST_H4, E> {
+    using G = E; using O = double; using X0 = E; using X1 = double; using X2 = double;
+    static constexpr int NX = 2; static constexpr bool FINAL = true; static constexpr bool EXACT = false;
+};
+template <typename E> struct StageT<ST_U1, E> {
+    using G = double; using O = double; using X0 = double; using X1 = double; using X2 = double;
+    static constexpr int NX = 0; static constexpr bool FINAL = false; static constexpr bool EXACT = true;
+};
+template <typename E> struct StageT<ST_U2, E> {
+    using G = double; using O = double; using X0 = double; using X1 = double; using X2 = double;
+    static constexpr int NX = 1; static constexpr bool FINAL = false; static constexpr bool EXACT = true;
+};
+template <typename E> struct StageT<ST_U3, E> : StageT<ST_U2, E> {};
+template <typename E> struct StageT<ST_U4, E> {
+    using G = double; using O = double; using X0 = double; using X1 = double; using X2 = double;
+    static constexpr int NX = 3; static constexpr bool FINAL = true; static constexpr bool EXACT = true;
+};
+
+struct TileCtrl {
+    uint64_t full[2], empty[2];
+    uint64_t rfull[kRingSlots], rempty[kRingSlots];
+    double wsum[kConsumerWarps];
+    double rates_d[kMaxR + 1];
+    float rates_f[kMaxR + 3];
+    int skip;
+    int err;
+    int is_last;
+    int pad;
+};
+constexpr int kCtrlBytes = 1024;
+static_assert(sizeof(TileCtrl) <= kCtrlBytes, "control block");
+
+template <int S, typename E> struct TileLayout {
+    using Tr = StageT<S, E>;
+    static constexpr int gb = kTile * sizeof(typename Tr::G);
+    static constexpr int x0b = Tr::NX > 0 ? kTile * sizeof(typename Tr::X0) : 0;
+    static constexpr int x1b = Tr::NX > 1 ? kTile * sizeof(typename Tr::X1) : 0;
+    static constexpr int x2b = Tr::NX > 2 ? kTile * sizeof(typename Tr::X2) : 0;
+    static constexpr int stage = gb + x0b + x1b + x2b;
+    static constexpr int bytes = kCtrlBytes + 2 * stage + kRingSlots * gb;
+};
+
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory"); }
+
+template <typename G> __device__ __forceinline__ G rate_of(const TileCtrl &c, int i);
+template <> __device__ __forceinline__ double rate_of<double>(const TileCtrl &c, int i) { return c.rates_d[i]; }
+template <> __device__ __forceinline__ float rate_of<float>(const TileCtrl &c, int i) { return c.rates_f[i]; }
+
+template <int S, typename E>
+__global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_constant__ TileParams p) {
+    using Tr = StageT<S, E>;
+    using G = typename Tr::G;
+    using O = typename Tr::O;
+    using X0 = typename Tr::X0;
+    using X1 = typename Tr::X1;
+    using X2 = typename Tr::X2;
+    using A = Ar<G, Tr::EXACT>;
+    using LY = TileLayout<S, E>;
+
+    extern __shared__ __align__(128) unsigned char tile_smem[];
+    TileCtrl &c = *reinterpret_cast<TileCtrl *>(tile_smem);
+    unsigned char *stage_base = tile_smem + kCtrlBytes;
+    unsigned char *ring_base = stage_base + 2 * LY::stage;
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int n = p.n;
+    const int ntb = n - kTileBits;  // tile-index bits (>= 1)
+
+    if (tid == 0) {
+        c.skip = (p.skip_if_done && p.ex) ? *reinterpret_cast<volatile int *>(&p.ex->done) : 0;
+        c.err = 0;
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&c.full[b], 1);
+            mbar_init(&c.empty[b], kConsumerWarps);
+        }
+        for (int s = 0; s < kRingSlots; ++s) {
+            mbar_init(&c.rfull[s], 1);
+            mbar_init(&c.rempty[s], kConsumerWarps);
+        }
+        fence_mbar_init();
+    }
+    if (tid <= n) {
+        const double r = rate_at(p.rs, tid, p.t);
+        c.rates_d[tid] = r;
+        c.rates_f[tid] = static_cast<float>(r);
+    }
+    __syncthreads();
+    if (c.skip) return;
+    volatile int *errf = &c.err;
+
+    const G *__restrict__ g = static_cast<const G *>(p.g);
+
+    if (warp == kConsumerWarps) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            const uint64_t keep = policy_evict_last();
+            const uint64_t once = policy_evict_first();
+            uint32_t it = 0, cur = 0;
+            bool ok = true;
+            for (unsigned long long T = blockIdx.x; T < p.ntiles && ok; T += gridDim.x, ++it) {
+                const int b = it & 1;
+                if (it >= 2 && !mbar_wait(&c.empty[b], ((it >> 1) - 1) & 1, errf)) break;
+                unsigned char *st = stage_base + b * LY::stage;
+                mbar_arrive_expect_tx(&c.full[b], LY::stage);
+                bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], keep);
+                if constexpr (Tr::NX > 0)
+                    bulk_g2s(st + LY::gb, static_cast<const X0 *>(p.s0) + T * kTile, LY::x0b, &c.full[b], once);
+                if constexpr (Tr::NX > 1)
+                    bulk_g2s(st + LY::gb + LY::x0b, static_cast<const X1 *>(p.s1) + T * kTile, LY::x1b,
+                             &c.full[b], once);
+                if constexpr (Tr::NX > 2)
+                    bulk_g2s(st + LY::gb + LY::x0b + LY::x1b, static_cast<const X2 *>(p.s2) + T * kTile,
+                             LY::x2b, &c.full[b], once);
+                // partner tiles, in the order the consumers add them
+                const bool top = (T >> (ntb - 1)) & 1;
+                const bool strad = !(T & 1);
+                const unsigned long long hmask =
+                    ntb >= 2 ? (T & ~(T >> 1) & ((1ull << (ntb - 1)) - 1)) : 0ull;
+                const int np = int(top) + int(strad) + __popcll(hmask);
+                unsigned long long hm = hmask;
+                for (int q = 0; q < np; ++q) {
+                    unsigned long long src;
+                    uint32_t bytes = LY::gb;
+                    if (q == 0 && top) {
+                        src = T - (1ull << (ntb - 1));
+                    } else if (q == int(top) && strad) {
+                        src = T + 1;
+                        bytes = LY::gb / 2;
+                    } else {
+                        const int u = __ffsll(hm) - 1;
+                        hm &= hm - 1;
+                        src = T + (1ull << u);
+                    }
+                    const int slot = cur % kRingSlots;
+                    if (cur >= kRingSlots && !mbar_wait(&c.rempty[slot], ((cur / kRingSlots) - 1) & 1, errf)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&c.rfull[slot], bytes);
+                    bulk_g2s(ring_base + slot * LY::gb, g + src * kTile, bytes, &c.rfull[slot], keep);
+                    ++cur;
+                }
+            }
+            if (!ok || *errf) {
+                atomicExch(&p.ex->error, 1);
+                // let every copy issued so far complete before the CTA can exit
+                for (int b = 0; b < 2; ++b) {
+                    const uint32_t uses = (it + 1 - b) / 2;  // tiles started on buffer b
+                    if (uses) mbar_drain(&c.full[b], (uses - 1) & 1, 100000000ull);
+                }
+                for (int s = 0; s < kRingSlots; ++s) {
+                    const uint32_t uses = cur > uint32_t(s) ? (cur - 1 - s) / kRingSlots + 1 : 0;
+                    if (uses) mbar_drain(&c.rfull[s], (uses - 1) & 1, 100000000ull);
+                }
+            }
+        }
+        return;
+    }
+
+    // ---------------- consumers ----------------
+    const G rn = rate_of<G>(c, n), r0 = rate_of<G>(c, 0), rn1 = rate_of<G>(c, n - 1), rn2 = rate_of<G>(c, n - 2);
+    const G rnL = rate_of<G>(c, n - kTileBits);
+    const uint64_t once = policy_evict_first();
+    O *__restrict__ out = static_cast<O *>(p.out);
+    double cs = 0.0;
+    uint32_t it = 0, cur = 0;
+    bool ok = true;
+
+    for (unsigned long long T = blockIdx.x; T < p.ntiles; T += gridDim.x, ++it) {
+        const int b = it & 1;
+        const bool top = (T >> (ntb - 1)) & 1;
+        const bool strad = !(T & 1);
+        const bool dstrad = (T & 1);
+        const unsigned long long lowmask = ntb >= 2 ? ((1ull << (ntb - 1)) - 1) : 0ull;
+        const unsigned long long hmask = T & ~(T >> 1) & lowmask;
+        const unsigned long long dhmask = ~T & (T >> 1) & lowmask;
+
+        G acc[2][4], xv[2][4];
+        const G *ent = nullptr;
+        int eslot = 0;
+        if (top) {
+            eslot = cur % kRingSlots;
+            if (!mbar_wait(&c.rfull[eslot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
+            ent = reinterpret_cast<const G *>(ring_base + eslot * LY::gb);
+        }
+        if (!mbar_wait(&c.full[b], (it >> 1) & 1, errf)) { ok = false; break; }
+        unsigned char *st = stage_base + b * LY::stage;
+        const G *xs = reinterpret_cast<const G *>(st);
+
+#pragma unroll
+        for (int gi = 0; gi < 2; ++gi) {
+            const uint32_t grp = tid + kConsumers * gi;
+            const int base = grp * 4;
+            G x0, x1, x2, x3;
+            V4<G>::lds(xs + base, x0, x1, x2, x3);
+            G a0 = G(0), a1 = G(0), a2 = G(0), a3 = G(0);
+            if (top) {  // 1. entry
+                G e0, e1, e2, e3;
+                V4<G>::lds(ent + base, e0, e1, e2, e3);
+                a0 = A::madd(a0, r0, e0); a1 = A::madd(a1, r0, e1);
+                a2 = A::madd(a2, r0, e2); a3 = A::madd(a3, r0, e3);
+            }
+            // 2. diagonal, subtraction order of src/lib/solv.c:103-116
+            G d0 = G(0), d1 = G(0), d2 = G(0), d3 = G(0);
+            d1 = A::sub(d1, rn); d3 = A::sub(d3, rn);                       // b0 set
+            if (!top) { d0 = A::sub(d0, r0); d1 = A::sub(d1, r0); d2 = A::sub(d2, r0); d3 = A::sub(d3, r0); }
+            d2 = A::sub(d2, rn1);                                           // j = 0
+            if (grp & 1) { d0 = A::sub(d0, rn2); d1 = A::sub(d1, rn2); }   // j = 1
+            uint32_t m = ~grp & (grp >> 1) & 0xFFu;                         // j = 2..9
+            while (m) {
+                const int q = __ffs(m) - 1;
+                m &= m - 1;
+                const G rr = rate_of<G>(c, n - 3 - q);
+                d0 = A::sub(d0, rr); d1 = A::sub(d1, rr); d2 = A::sub(d2, rr); d3 = A::sub(d3, rr);
+            }
+            if (!(grp >> 8) && dstrad) {                                    // j = 10
+                d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL); d2 = A::sub(d2, rnL); d3 = A::sub(d3, rnL);
+            }
+            unsigned long long mh = dhmask;                                 // j >= 11
+            while (mh) {
+                const int u = __ffsll(mh) - 1;
+                mh &= mh - 1;
+                const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
+                d0 = A::sub(d0, rr); d1 = A::sub(d1, rr); d2 = A::sub(d2, rr); d3 = A::sub(d3, rr);
+            }
+            a0 = A::madd(a0, d0, x0); a1 = A::madd(a1, d1, x1);
+            a2 = A::madd(a2, d2, x2); a3 = A::madd(a3, d3, x3);
+            // 3. exit (b0 clear: states 0 and 2 of the group)
+            a0 = A::madd(a0, rn, x1);
+            a2 = A::madd(a2, rn, x3);
+            // 4. hops, ascending bit
+            a1 = A::madd(a1, rn1, x2);                                      // k = 0
+            if (!(grp & 1)) {                                               // k = 1
+                G p0, p1;
+                V4<G>::lds2(xs + base + 4, p0, p1);
+                a2 = A::madd(a2, rn2, p0);
+                a3 = A::madd(a3, rn2, p1);
+            }
+            uint32_t hm = grp & ~(grp >> 1) & 0xFFu;                        // k = 2..9
+            while (hm) {
+                const int q = __ffs(hm) - 1;
+                hm &= hm - 1;
+                const G rr = rate_of<G>(c, n - 3 - q);
+                G p0, p1, p2, p3;
+                V4<G>::lds(xs + base + (4 << q), p0, p1, p2, p3);
+                a0 = A::madd(a0, rr, p0); a1 = A::madd(a1, rr, p1);
+                a2 = A::madd(a2, rr, p2); a3 = A::madd(a3, rr, p3);
+            }
+            acc[gi][0] = a0; acc[gi][1] = a1; acc[gi][2] = a2; acc[gi][3] = a3;
+            xv[gi][0] = x0; xv[gi][1] = x1; xv[gi][2] = x2; xv[gi][3] = x3;
+        }
+        if (top) {
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&c.rempty[eslot]);
+            ++cur;
+        }
+        if (strad) {  // k = 10: upper half of this tile <- lower half of tile T+1
+            const int slot = cur % kRingSlots;
+            if (!mbar_wait(&c.rfull[slot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
+            const G *hp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
+            G p0, p1, p2, p3;
+            V4<G>::lds(hp + 4 * tid, p0, p1, p2, p3);
+            acc[1][0] = A::madd(acc[1][0], rnL, p0); acc[1][1] = A::madd(acc[1][1], rnL, p1);
+            acc[1][2] = A::madd(acc[1][2], rnL, p2); acc[1][3] = A::madd(acc[1][3], rnL, p3);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&c.rempty[slot]);
+            ++cur;
+        }
+        {
+            unsigned long long mh = hmask;  // k >= 11
+            while (mh) {
+                const int u = __ffsll(mh) - 1;
+                mh &= mh - 1;
+                const int slot = cur % kRingSlots;
+                if (!mbar_wait(&c.rfull[slot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
+                const G *pp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
+                const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
+#pragma unroll
+                for (int gi = 0; gi < 2; ++gi) {
+                    G p0, p1, p2, p3;
+                    V4<G>::lds(pp + 4 * (tid + kConsumers * gi), p0, p1, p2, p3);
+                    acc[gi][0] = A::madd(acc[gi][0], rr, p0); acc[gi][1] = A::madd(acc[gi][1], rr, p1);
+                    acc[gi][2] = A::madd(acc[gi][2], rr, p2); acc[gi][3] = A::madd(acc[gi][3], rr, p3);
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&c.rempty[slot]);
+                ++cur;
+            }
+            if (!ok) break;
+        }
+
+        // ---- epilogue ----
+        const X0 *xa = reinterpret_cast<const X0 *>(st + LY::gb);
+        const X1 *xb = reinterpret_cast<const X1 *>(st + LY::gb + LY::x0b);
+        const X2 *xc = reinterpret_cast<const X2 *>(st + LY::gb + LY::x0b + LY::x1b);
+#pragma unroll
+        for (int gi = 0; gi < 2; ++gi) {
+            const int base = 4 * (tid + kConsumers * gi);
+            O o[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const G Tv = acc[gi][j];
+                if constexpr (S == ST_APPLY) {
+                    o[j] = Tv;
+                } else if constexpr (S == ST_REF) {
+                    const double kv = __dmul_rn(p.h, Tv);
+                    const double k2 = __dmul_rn(2.0, kv);
+                    const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv), 6.0);
+                    o[j] = __dadd_rn(xv[gi][j], D);
+                    cs += fabs(D);
+                } else if constexpr (S == ST_H1) {
+                    o[j] = static_cast<O>(p.h * Tv);
+                } else if constexpr (S == ST_H2) {
+                    o[j] = static_cast<O>(xv[gi][j] + static_cast<G>(p.hc) * Tv);
+                } else if constexpr (S == ST_H3) {
+                    o[j] = static_cast<O>(xa[base + j] + static_cast<G>(p.hc) * Tv);
+                } else if constexpr (S == ST_H4) {
+                    const double D = static_cast<double>(xa[base + j]) + p.hc * static_cast<double>(Tv);
+                    o[j] = xb[base + j] + D;
+                    cs += fabs(D);
+                } else if constexpr (S == ST_U1) {
+                    o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xv[gi][j]);
+                } else if constexpr (S == ST_U2 || S == ST_U3) {
+                    o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xa[base + j]);
+                } else if constexpr (S == ST_U4) {
+                    const double x = xa[base + j];
+                    const double k1 = 2.0 * (xb[base + j] - x);
+                    const double k2 = 2.0 * (xc[base + j] - x);
+                    const double k3 = xv[gi][j] - x;
+                    const double k4 = __dmul_rn(p.h, Tv);
+                    const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4), 6.0);
+                    o[j] = __dadd_rn(x, D);
+                    cs += fabs(D);
+                }
+            }
+            V4<O>::stg(out + T * kTile + base, o[0], o[1], o[2], o[3], once);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&c.empty[b]);
+    }
+    if (!ok || *errf) atomicExch(&p.ex->error, 1);
+
+    if constexpr (Tr::FINAL) {
+        // deterministic CTA sum, then the last CTA reduces all partials in
+        // CTA order and applies the exit rule (src/masterEquation.c:670-679)
+        const double ws = warp_sum(cs);
+        if (lane == 0) c.wsum[warp] = ws;
+        consumer_sync();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int w = 0; w < kConsumerWarps; ++w) s += c.wsum[w];
+            p.partials[blockIdx.x] = s;
+            __threadfence();
+            const unsigned t = atomicAdd(p.counter, 1u);
+            c.is_last = (t == gridDim.x - 1);
+        }
+        consumer_sync();
+        if (c.is_last && warp == 0) {
+            __threadfence();
+            double s = 0.0;
+            for (unsigned i = lane; i < gridDim.x; i += 32) s += __ldcg(p.partials + i);
+            s = warp_sum(s);
+            if (lane == 0) {
+                ExitState *ex = p.ex;
+                ex->last_checksum = s;
+                ex->steps_done = p.step + 1;
+                if (p.exit_rule) {
+                    if (s < p.thresh) {
+                        ex->early_stop += 1;
+                        ex->steps_at_stop = p.step;
+                    } else {
+                        ex->early_stop = 0;
+                    }
+                    if (ex->early_stop > p.stop_count) {
+                        ex->done = 1;
+                        ex->converged = 1;
+                    }
+                }
+                *p.counter = 0u;
+                __threadfence();
+            }
+        }
+    }
+}
+
+}  // namespace tasep

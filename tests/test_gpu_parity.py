@@ -1,0 +1,183 @@
+"""GPU parity: the sm_100a kernels against the CPU oracle, through the C ABI.
+
+Tolerances (from the integrator spec): probabilities within 1e-12 absolute,
+expectations within 1e-12 relative.  The reference-compatible integrator
+(REF) and the generator product are held to bit equality with the oracle,
+which is itself bit-equal to the reference's compiled step code
+(tests/test_oracle_golden.py).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import tasep_b200 as T
+
+pytestmark = pytest.mark.gpu
+
+PROB_TOL = 1e-12
+EXP_RTOL = 1e-12
+
+
+def rates_for(n, seed):
+    rng = np.random.default_rng(seed)
+    r = np.empty(n + 1)
+    r[0], r[n] = rng.uniform(0.1, 1.0, 2)
+    r[1:n] = np.clip(rng.lognormal(0.0, 0.5, n - 1), 0.1, 5.0)
+    return r
+
+
+def torch_dev():
+    import torch
+    assert torch.cuda.is_available(), "CUDA device required"
+    return torch
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 7, 10, 11, 12, 13, 14, 16, 19])
+def test_apply_bit_exact(n):
+    torch = torch_dev()
+    rng = np.random.default_rng(100 + n)
+    r = rates_for(n, n)
+    x = rng.random(1 << n)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty_like(xd)
+    T.apply_device(n, r, xd.data_ptr(), yd.data_ptr())
+    torch.cuda.synchronize()
+    y = yd.cpu().numpy()
+    yo = O.apply(n, r, x)
+    assert np.array_equal(y, yo), f"max diff {np.max(np.abs(y - yo))}"
+    # generator columns sum to zero: 1^T M x = 0
+    assert abs(y.sum()) < 1e-12 * max(1.0, np.abs(y).sum())
+
+
+@pytest.mark.parametrize("n", [3, 11, 12, 15])
+def test_step_ref_device_bit_exact(n):
+    torch = torch_dev()
+    rng = np.random.default_rng(7 + n)
+    r = rates_for(n, 2 * n)
+    x = rng.random(1 << n)
+    x /= x.sum()
+    xd = torch.from_numpy(x).cuda()
+    od = torch.empty_like(xd)
+    cs = T.step_ref_device(n, r, 0.01, xd.data_ptr(), od.data_ptr())
+    xo = x.copy()
+    cso = O.step_ref(n, r, 0.01, xo)
+    assert np.array_equal(od.cpu().numpy(), xo)
+    assert cs == pytest.approx(cso, rel=1e-13)
+
+
+@pytest.mark.parametrize("n,init", [(4, O.INIT_EMPTY), (6, O.INIT_UNIFORM), (10, O.INIT_EMPTY),
+                                    (12, O.INIT_EMPTY), (13, O.INIT_UNIFORM), (14, O.INIT_EMPTY)])
+def test_run_ref_matches_oracle(n, init):
+    r = rates_for(n, 30 + n)
+    steps = 3000 if n <= 12 else 400
+    xo, ro = O.run(n, r, h=0.01, steps=steps, init=init, stop_tol=1e-7)
+    with T.Meq(n, T.INTEGRATOR_REF) as m:
+        m.set_rates(r)
+        m.init(init)
+        res = m.run(0.01, steps, stop_tol=1e-7)
+        x = m.store()
+    assert res["steps_done"] == ro["steps_done"]
+    assert res["early_stop"] == ro["early_stop"]
+    assert np.array_equal(x, xo), f"max diff {np.max(np.abs(x - xo))}"
+    assert res["last_checksum"] == pytest.approx(ro["last_checksum"], rel=1e-12)
+
+
+def test_run_ref_converges_like_reference_config1():
+    """n=10, alpha=.6, beta=.4, gamma=1, uniform start, coded 1e-7 rule:
+    the reference converges after step 20935 (exit on the 101st qualifying step)."""
+    n = 10
+    r = np.array([0.6] + [1.0] * 9 + [0.4])
+    xo, ro = O.run(n, r, h=0.01, steps=30000, init=O.INIT_UNIFORM, stop_tol=1e-7)
+    with T.Meq(n, T.INTEGRATOR_REF) as m:
+        m.set_rates(r)
+        m.init(T.INIT_UNIFORM)
+        res = m.run(0.01, 30000, stop_tol=1e-7)
+        x = m.store()
+    assert ro["steps_at_stop"] == 20935
+    assert res["steps_at_stop"] == 20935 and res["steps_done"] == 20936
+    assert np.array_equal(x, xo)
+
+
+@pytest.mark.parametrize("n", [5, 10, 12, 14, 16])
+def test_run_rk4_fp64(n):
+    r = rates_for(n, 50 + n)
+    steps = 600
+    xo, ro = O.run(n, r, h=0.01, steps=steps, integrator=O.INT_RK4, init=O.INIT_EMPTY, exit_rule=False)
+    with T.Meq(n, T.INTEGRATOR_RK4) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res = m.run(0.01, steps, exit_rule=False)
+        x = m.store()
+        obs = m.observables()
+    assert res["steps_done"] == steps
+    assert np.max(np.abs(x - xo)) <= PROB_TOL
+    yo = O.densities(n, xo)
+    assert np.allclose(obs["rho"], yo, rtol=EXP_RTOL, atol=0)
+    assert res["last_checksum"] == pytest.approx(ro["last_checksum"], rel=1e-9)
+
+
+@pytest.mark.parametrize("n", [8, 13])
+def test_run_rk4_to_steady_state_exit_rule(n):
+    r = rates_for(n, 70 + n)
+    xo, ro = O.run(n, r, h=0.01, steps=200000, integrator=O.INT_RK4, init=O.INIT_EMPTY, stop_tol=1e-10)
+    with T.Meq(n, T.INTEGRATOR_RK4) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res = m.run(0.01, 200000, stop_tol=1e-10)
+        x = m.store()
+    assert ro["early_stop"] == 101 and res["converged"] == 1
+    assert abs(int(res["steps_done"]) - int(ro["steps_done"])) <= 2
+    assert np.max(np.abs(x - xo)) <= 1e-12
+
+
+@pytest.mark.parametrize("n,integrator", [(6, O.INT_REF), (6, O.INT_RK4), (13, O.INT_REF), (13, O.INT_RK4)])
+def test_timevar(n, integrator):
+    rng = np.random.default_rng(5)
+    base = rates_for(n, 90 + n)
+    tv = {"type": rng.integers(0, 3, n + 1), "amplitude": 0.5 * base, "period": rng.uniform(0.5, 2, n + 1),
+          "offset": rng.uniform(0, 1, n + 1), "constant": base}
+    steps = 500
+    xo, ro = O.run(n, base, h=0.01, steps=steps, integrator=integrator, init=O.INIT_EMPTY, timevar=tv,
+                   exit_rule=False)
+    with T.Meq(n, integrator) as m:
+        m.set_rates(base)
+        m.set_timevar(tv["type"], tv["amplitude"], tv["period"], tv["offset"], tv["constant"])
+        m.init(T.INIT_EMPTY)
+        res = m.run(0.01, steps, exit_rule=False)
+        x = m.store()
+    assert res["steps_done"] == steps
+    assert np.max(np.abs(x - xo)) <= PROB_TOL
+
+
+@pytest.mark.parametrize("n", [9, 14])
+def test_mixed_precision_steady_state(n):
+    r = rates_for(n, 110 + n)
+    xo, ro = O.run(n, r, h=0.01, steps=200000, integrator=O.INT_RK4, init=O.INIT_EMPTY, stop_tol=1e-10)
+    with T.Meq(n, T.INTEGRATOR_RK4, T.PRECISION_MIXED) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res = m.run(0.01, 200000, stop_tol=1e-10)
+        obs = m.observables()
+    assert res["converged"] == 1
+    yo = O.densities(n, xo)
+    assert np.max(np.abs(obs["rho"] - yo)) <= 1e-6
+    assert abs(obs["mass"] - 1.0) <= 1e-9
+
+
+@pytest.mark.parametrize("n", [2, 4, 9, 11, 12, 15, 17])
+def test_observables(n):
+    rng = np.random.default_rng(n)
+    x = rng.random(1 << n)
+    x /= x.sum()
+    with T.Meq(n, T.INTEGRATOR_REF) as m:
+        m.set_rates(rates_for(n, 1))
+        m.load(x)
+        obs = m.observables()
+    yo = O.densities(n, x)
+    cov, mul = O.covariance(n, x, yo)
+    assert np.allclose(obs["rho"], yo, rtol=EXP_RTOL, atol=0)
+    assert np.max(np.abs(obs["cov"] - cov)) <= 1e-13
+    assert np.max(np.abs(obs["mul"] - mul)) <= 1e-13
+    assert obs["mass"] == pytest.approx(x.sum(), rel=1e-14)
+    if n >= 4:
+        assert np.max(np.abs(obs["window4"] - O.window4(n, x))) <= 1e-14
