@@ -12,17 +12,21 @@
 //   4. hops from i + 2^k for k ascending where b_k & !b_(k+1), rate r[n-1-k].
 //
 // Layout: the state vector is one flat array in reference index order.  A
-// tile is 2^kTileBits consecutive states; tile T's high bits are the state's
-// bits >= kTileBits.  Per CTA (one per SM, persistent):
+// tile is 2^kTileBits consecutive states; tile T's index holds the state's
+// bits >= kTileBits.  Per CTA (one per SM, persistent over tiles):
 //   * a producer warp streams, with cp.async.bulk (no multicast), the tile of
 //     g and of each per-state extra input into a double-buffered stage, then
 //     every partner tile this tile needs - the entry tile, the lower half of
-//     tile T+1 (the hop straddling the tile boundary) and one tile per active
-//     high hop - into a ring of shared-memory slots;
-//   * 8 consumer warps own 4 consecutive states per group, 2 groups each.
-//     Hops inside a group are register moves, hops between groups read the
-//     staged tile, high hops read the ring slots in ascending bit order, so
-//     the reference's summation order is kept exactly.
+//     tile T+1 (the hop straddling the tile edge) and one tile per active high
+//     hop - into a ring of shared-memory slots;
+//   * 16 consumer warps own one group of 4 consecutive states per thread.
+//     Hops inside a group are register moves; hops between groups read the
+//     staged tile with predicated loads (fully unrolled, so independent chains
+//     interleave); high hops read the ring slots in ascending bit order.  The
+//     diagonal's low part (everything up to bit 9, which precedes the tile-
+//     level terms in the reference's subtraction order) comes from a table
+//     built once per launch, the remaining terms are subtracted in order, so
+//     the reference's rounding sequence is kept exactly.
 // Tiles are visited in natural order by all CTAs together, so partner tiles
 // up to a few tens of MB ahead are still in L2 when they are gathered.
 #pragma once
@@ -33,11 +37,11 @@ namespace tasep {
 
 constexpr int kTileBits = 11;
 constexpr int kTile = 1 << kTileBits;               // states per tile
-constexpr int kConsumerWarps = 8;
-constexpr int kConsumers = kConsumerWarps * 32;      // 256
+constexpr int kConsumerWarps = 16;
+constexpr int kConsumers = kConsumerWarps * 32;      // 512: one group of 4 states each
 constexpr int kTileThreads = kConsumers + 32;        // + producer warp
 constexpr int kRingSlots = 4;
-static_assert(kTile / 4 == 2 * kConsumers, "two groups of four states per consumer thread");
+static_assert(kTile / 4 == kConsumers, "one group of four states per consumer thread");
 
 struct TileParams {
     int n;
@@ -119,7 +123,8 @@ template <int S, typename E> struct TileLayout {
     static constexpr int x1b = Tr::NX > 1 ? kTile * sizeof(typename Tr::X1) : 0;
     static constexpr int x2b = Tr::NX > 2 ? kTile * sizeof(typename Tr::X2) : 0;
     static constexpr int stage = gb + x0b + x1b + x2b;
-    static constexpr int bytes = kCtrlBytes + 2 * stage + kRingSlots * gb;
+    static constexpr int dtab = 2 * gb;  // low diagonal prefixes, for top bit clear / set
+    static constexpr int bytes = kCtrlBytes + 2 * stage + kRingSlots * gb + dtab;
 };
 
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory"); }
@@ -143,6 +148,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     TileCtrl &c = *reinterpret_cast<TileCtrl *>(tile_smem);
     unsigned char *stage_base = tile_smem + kCtrlBytes;
     unsigned char *ring_base = stage_base + 2 * LY::stage;
+    G *dtab = reinterpret_cast<G *>(ring_base + kRingSlots * LY::gb);
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -241,10 +247,30 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     }
 
     // ---------------- consumers ----------------
+    // Low diagonal prefixes: d = 0; -r[n] if b0; -r[0] if top clear; then
+    // -r[n-1-j] for j = 0..9 where b_j = 0, b_(j+1) = 1 (src/lib/solv.c:103-116).
+    for (int l = tid; l < kTile; l += kConsumers) {
+        for (int tp = 0; tp < 2; ++tp) {
+            G d = G(0);
+            if (l & 1) d = A::sub(d, rate_of<G>(c, n));
+            if (!tp) d = A::sub(d, rate_of<G>(c, 0));
+            for (int j = 0; j < kTileBits - 1; ++j)
+                if (!((l >> j) & 1) && ((l >> (j + 1)) & 1)) d = A::sub(d, rate_of<G>(c, n - 1 - j));
+            dtab[tp * kTile + l] = d;
+        }
+    }
     const G rn = rate_of<G>(c, n), r0 = rate_of<G>(c, 0), rn1 = rate_of<G>(c, n - 1), rn2 = rate_of<G>(c, n - 2);
     const G rnL = rate_of<G>(c, n - kTileBits);
+    G rq[kTileBits - 3];  // hop k = q + 2 uses r[n-3-q]
+#pragma unroll
+    for (int q = 0; q < kTileBits - 3; ++q) rq[q] = rate_of<G>(c, n - 3 - q);
+    consumer_sync();
+
     const uint64_t once = policy_evict_first();
     O *__restrict__ out = static_cast<O *>(p.out);
+    const uint32_t grp = tid;          // group of 4 states: local states 4*grp .. 4*grp+3
+    const int base = 4 * tid;
+    const bool hi10 = (grp >> 8) & 1;  // state bit 10 (warp-uniform)
     double cs = 0.0;
     uint32_t it = 0, cur = 0;
     bool ok = true;
@@ -253,98 +279,79 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         const int b = it & 1;
         const bool top = (T >> (ntb - 1)) & 1;
         const bool strad = !(T & 1);
-        const bool dstrad = (T & 1);
         const unsigned long long lowmask = ntb >= 2 ? ((1ull << (ntb - 1)) - 1) : 0ull;
         const unsigned long long hmask = T & ~(T >> 1) & lowmask;
         const unsigned long long dhmask = ~T & (T >> 1) & lowmask;
 
-        G acc[2][4], xv[2][4];
-        const G *ent = nullptr;
+        G a0 = G(0), a1 = G(0), a2 = G(0), a3 = G(0);
         int eslot = 0;
-        if (top) {
+        if (top) {  // 1. entry
             eslot = cur % kRingSlots;
             if (!mbar_wait(&c.rfull[eslot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
-            ent = reinterpret_cast<const G *>(ring_base + eslot * LY::gb);
+            const G *ent = reinterpret_cast<const G *>(ring_base + eslot * LY::gb);
+            G e0, e1, e2, e3;
+            V4<G>::lds(ent + base, e0, e1, e2, e3);
+            a0 = A::madd(a0, r0, e0); a1 = A::madd(a1, r0, e1);
+            a2 = A::madd(a2, r0, e2); a3 = A::madd(a3, r0, e3);
+            ++cur;  // the slot is released after the in-tile terms below
         }
         if (!mbar_wait(&c.full[b], (it >> 1) & 1, errf)) { ok = false; break; }
         unsigned char *st = stage_base + b * LY::stage;
         const G *xs = reinterpret_cast<const G *>(st);
 
-#pragma unroll
-        for (int gi = 0; gi < 2; ++gi) {
-            const uint32_t grp = tid + kConsumers * gi;
-            const int base = grp * 4;
-            G x0, x1, x2, x3;
-            V4<G>::lds(xs + base, x0, x1, x2, x3);
-            G a0 = G(0), a1 = G(0), a2 = G(0), a3 = G(0);
-            if (top) {  // 1. entry
-                G e0, e1, e2, e3;
-                V4<G>::lds(ent + base, e0, e1, e2, e3);
-                a0 = A::madd(a0, r0, e0); a1 = A::madd(a1, r0, e1);
-                a2 = A::madd(a2, r0, e2); a3 = A::madd(a3, r0, e3);
-            }
-            // 2. diagonal, subtraction order of src/lib/solv.c:103-116
-            G d0 = G(0), d1 = G(0), d2 = G(0), d3 = G(0);
-            d1 = A::sub(d1, rn); d3 = A::sub(d3, rn);                       // b0 set
-            if (!top) { d0 = A::sub(d0, r0); d1 = A::sub(d1, r0); d2 = A::sub(d2, r0); d3 = A::sub(d3, r0); }
-            d2 = A::sub(d2, rn1);                                           // j = 0
-            if (grp & 1) { d0 = A::sub(d0, rn2); d1 = A::sub(d1, rn2); }   // j = 1
-            uint32_t m = ~grp & (grp >> 1) & 0xFFu;                         // j = 2..9
-            while (m) {
-                const int q = __ffs(m) - 1;
-                m &= m - 1;
-                const G rr = rate_of<G>(c, n - 3 - q);
-                d0 = A::sub(d0, rr); d1 = A::sub(d1, rr); d2 = A::sub(d2, rr); d3 = A::sub(d3, rr);
-            }
-            if (!(grp >> 8) && dstrad) {                                    // j = 10
-                d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL); d2 = A::sub(d2, rnL); d3 = A::sub(d3, rnL);
-            }
-            unsigned long long mh = dhmask;                                 // j >= 11
+        G x0, x1, x2, x3;
+        V4<G>::lds(xs + base, x0, x1, x2, x3);
+        // 2. diagonal: low prefix from the table, then j = 10 and j >= 11
+        G d0, d1, d2, d3;
+        V4<G>::lds(dtab + (top ? kTile : 0) + base, d0, d1, d2, d3);
+        if (!hi10 && !strad) {  // j = 10: b10 = 0, b11 = 1
+            d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL); d2 = A::sub(d2, rnL); d3 = A::sub(d3, rnL);
+        }
+        {
+            unsigned long long mh = dhmask;
             while (mh) {
                 const int u = __ffsll(mh) - 1;
                 mh &= mh - 1;
                 const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 d0 = A::sub(d0, rr); d1 = A::sub(d1, rr); d2 = A::sub(d2, rr); d3 = A::sub(d3, rr);
             }
-            a0 = A::madd(a0, d0, x0); a1 = A::madd(a1, d1, x1);
-            a2 = A::madd(a2, d2, x2); a3 = A::madd(a3, d3, x3);
-            // 3. exit (b0 clear: states 0 and 2 of the group)
-            a0 = A::madd(a0, rn, x1);
-            a2 = A::madd(a2, rn, x3);
-            // 4. hops, ascending bit
-            a1 = A::madd(a1, rn1, x2);                                      // k = 0
-            if (!(grp & 1)) {                                               // k = 1
-                G p0, p1;
-                V4<G>::lds2(xs + base + 4, p0, p1);
-                a2 = A::madd(a2, rn2, p0);
-                a3 = A::madd(a3, rn2, p1);
-            }
-            uint32_t hm = grp & ~(grp >> 1) & 0xFFu;                        // k = 2..9
-            while (hm) {
-                const int q = __ffs(hm) - 1;
-                hm &= hm - 1;
-                const G rr = rate_of<G>(c, n - 3 - q);
+        }
+        a0 = A::madd(a0, d0, x0); a1 = A::madd(a1, d1, x1);
+        a2 = A::madd(a2, d2, x2); a3 = A::madd(a3, d3, x3);
+        // 3. exit (b0 clear: states 0 and 2 of the group)
+        a0 = A::madd(a0, rn, x1);
+        a2 = A::madd(a2, rn, x3);
+        // 4. hops, ascending bit
+        a1 = A::madd(a1, rn1, x2);  // k = 0
+        if (!(grp & 1)) {           // k = 1
+            G p0, p1;
+            V4<G>::lds2(xs + base + 4, p0, p1);
+            a2 = A::madd(a2, rn2, p0);
+            a3 = A::madd(a3, rn2, p1);
+        }
+#pragma unroll
+        for (int q = 0; q < kTileBits - 3; ++q) {  // k = q + 2 = 2..9
+            if (((grp >> q) & 3u) == 1u) {
                 G p0, p1, p2, p3;
                 V4<G>::lds(xs + base + (4 << q), p0, p1, p2, p3);
-                a0 = A::madd(a0, rr, p0); a1 = A::madd(a1, rr, p1);
-                a2 = A::madd(a2, rr, p2); a3 = A::madd(a3, rr, p3);
+                a0 = A::madd(a0, rq[q], p0); a1 = A::madd(a1, rq[q], p1);
+                a2 = A::madd(a2, rq[q], p2); a3 = A::madd(a3, rq[q], p3);
             }
-            acc[gi][0] = a0; acc[gi][1] = a1; acc[gi][2] = a2; acc[gi][3] = a3;
-            xv[gi][0] = x0; xv[gi][1] = x1; xv[gi][2] = x2; xv[gi][3] = x3;
         }
         if (top) {
             __syncwarp();
             if (lane == 0) mbar_arrive(&c.rempty[eslot]);
-            ++cur;
         }
         if (strad) {  // k = 10: upper half of this tile <- lower half of tile T+1
             const int slot = cur % kRingSlots;
             if (!mbar_wait(&c.rfull[slot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
-            const G *hp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
-            G p0, p1, p2, p3;
-            V4<G>::lds(hp + 4 * tid, p0, p1, p2, p3);
-            acc[1][0] = A::madd(acc[1][0], rnL, p0); acc[1][1] = A::madd(acc[1][1], rnL, p1);
-            acc[1][2] = A::madd(acc[1][2], rnL, p2); acc[1][3] = A::madd(acc[1][3], rnL, p3);
+            if (hi10) {
+                const G *hp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
+                G p0, p1, p2, p3;
+                V4<G>::lds(hp + base - kTile / 2, p0, p1, p2, p3);
+                a0 = A::madd(a0, rnL, p0); a1 = A::madd(a1, rnL, p1);
+                a2 = A::madd(a2, rnL, p2); a3 = A::madd(a3, rnL, p3);
+            }
             __syncwarp();
             if (lane == 0) mbar_arrive(&c.rempty[slot]);
             ++cur;
@@ -358,13 +365,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 if (!mbar_wait(&c.rfull[slot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
                 const G *pp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
                 const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
-#pragma unroll
-                for (int gi = 0; gi < 2; ++gi) {
-                    G p0, p1, p2, p3;
-                    V4<G>::lds(pp + 4 * (tid + kConsumers * gi), p0, p1, p2, p3);
-                    acc[gi][0] = A::madd(acc[gi][0], rr, p0); acc[gi][1] = A::madd(acc[gi][1], rr, p1);
-                    acc[gi][2] = A::madd(acc[gi][2], rr, p2); acc[gi][3] = A::madd(acc[gi][3], rr, p3);
-                }
+                G p0, p1, p2, p3;
+                V4<G>::lds(pp + base, p0, p1, p2, p3);
+                a0 = A::madd(a0, rr, p0); a1 = A::madd(a1, rr, p1);
+                a2 = A::madd(a2, rr, p2); a3 = A::madd(a3, rr, p3);
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&c.rempty[slot]);
                 ++cur;
@@ -376,48 +380,46 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         const X0 *xa = reinterpret_cast<const X0 *>(st + LY::gb);
         const X1 *xb = reinterpret_cast<const X1 *>(st + LY::gb + LY::x0b);
         const X2 *xc = reinterpret_cast<const X2 *>(st + LY::gb + LY::x0b + LY::x1b);
+        const G acc[4] = {a0, a1, a2, a3};
+        const G xv[4] = {x0, x1, x2, x3};
+        O o[4];
 #pragma unroll
-        for (int gi = 0; gi < 2; ++gi) {
-            const int base = 4 * (tid + kConsumers * gi);
-            O o[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const G Tv = acc[gi][j];
-                if constexpr (S == ST_APPLY) {
-                    o[j] = Tv;
-                } else if constexpr (S == ST_REF) {
-                    const double kv = __dmul_rn(p.h, Tv);
-                    const double k2 = __dmul_rn(2.0, kv);
-                    const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv), 6.0);
-                    o[j] = __dadd_rn(xv[gi][j], D);
-                    cs += fabs(D);
-                } else if constexpr (S == ST_H1) {
-                    o[j] = static_cast<O>(p.h * Tv);
-                } else if constexpr (S == ST_H2) {
-                    o[j] = static_cast<O>(xv[gi][j] + static_cast<G>(p.hc) * Tv);
-                } else if constexpr (S == ST_H3) {
-                    o[j] = static_cast<O>(xa[base + j] + static_cast<G>(p.hc) * Tv);
-                } else if constexpr (S == ST_H4) {
-                    const double D = static_cast<double>(xa[base + j]) + p.hc * static_cast<double>(Tv);
-                    o[j] = xb[base + j] + D;
-                    cs += fabs(D);
-                } else if constexpr (S == ST_U1) {
-                    o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xv[gi][j]);
-                } else if constexpr (S == ST_U2 || S == ST_U3) {
-                    o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xa[base + j]);
-                } else if constexpr (S == ST_U4) {
-                    const double x = xa[base + j];
-                    const double k1 = 2.0 * (xb[base + j] - x);
-                    const double k2 = 2.0 * (xc[base + j] - x);
-                    const double k3 = xv[gi][j] - x;
-                    const double k4 = __dmul_rn(p.h, Tv);
-                    const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4), 6.0);
-                    o[j] = __dadd_rn(x, D);
-                    cs += fabs(D);
-                }
+        for (int j = 0; j < 4; ++j) {
+            const G Tv = acc[j];
+            if constexpr (S == ST_APPLY) {
+                o[j] = Tv;
+            } else if constexpr (S == ST_REF) {
+                const double kv = __dmul_rn(p.h, Tv);
+                const double k2 = __dmul_rn(2.0, kv);
+                const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv), 6.0);
+                o[j] = __dadd_rn(xv[j], D);
+                cs += fabs(D);
+            } else if constexpr (S == ST_H1) {
+                o[j] = static_cast<O>(p.h * Tv);
+            } else if constexpr (S == ST_H2) {
+                o[j] = static_cast<O>(xv[j] + static_cast<G>(p.hc) * Tv);
+            } else if constexpr (S == ST_H3) {
+                o[j] = static_cast<O>(xa[base + j] + static_cast<G>(p.hc) * Tv);
+            } else if constexpr (S == ST_H4) {
+                const double D = static_cast<double>(xa[base + j]) + p.hc * static_cast<double>(Tv);
+                o[j] = xb[base + j] + D;
+                cs += fabs(D);
+            } else if constexpr (S == ST_U1) {
+                o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xv[j]);
+            } else if constexpr (S == ST_U2 || S == ST_U3) {
+                o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xa[base + j]);
+            } else if constexpr (S == ST_U4) {
+                const double x = xa[base + j];
+                const double k1 = 2.0 * (xb[base + j] - x);
+                const double k2 = 2.0 * (xc[base + j] - x);
+                const double k3 = xv[j] - x;
+                const double k4 = __dmul_rn(p.h, Tv);
+                const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4), 6.0);
+                o[j] = __dadd_rn(x, D);
+                cs += fabs(D);
             }
-            V4<O>::stg(out + T * kTile + base, o[0], o[1], o[2], o[3], once);
         }
+        V4<O>::stg(out + T * kTile + base, o[0], o[1], o[2], o[3], once);
         __syncwarp();
         if (lane == 0) mbar_arrive(&c.empty[b]);
     }
