@@ -134,6 +134,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
     }
 }
 
+// Hands a shared-memory buffer back to the bulk-copy producer.  The reads of
+// the buffer were generic-proxy loads and the producer's next bulk copy into
+// it is an async-proxy write: every reading thread fences the two proxies
+// before the warp arrives, otherwise the copy can overwrite data a lane has
+// not finished reading (seen as stale partner tiles under load).
+__device__ __forceinline__ void consumer_release(uint64_t *bar, int lane) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) mbar_arrive(bar);
+}
+
 // Bounded wait that ignores the error flag: used on the error path to let
 // copies already issued land before the CTA exits.
 __device__ __forceinline__ void mbar_drain(uint64_t *bar, uint32_t parity, uint64_t limit_ns) {
@@ -176,6 +187,17 @@ template <> struct V4<double> {
         const double2 u = reinterpret_cast<const double2 *>(p)[0];
         a = u.x; b = u.y;
     }
+    // read-once coherent global load (no L1 allocation, evict-first in L2).  Not
+    // the .nc path: the stage that reads the state also rewrites it in place.
+    static __device__ __forceinline__ void ldg(const double *p, double &a, double &b, double &c, double &d,
+                                               uint64_t pol) {
+        asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+                     : "=d"(a), "=d"(b)
+                     : "l"(p), "l"(pol));
+        asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+                     : "=d"(c), "=d"(d)
+                     : "l"(p + 2), "l"(pol));
+    }
     static __device__ __forceinline__ void stg(double *p, double a, double b, double c, double d, uint64_t pol) {
         asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(a), "d"(b),
                      "l"(pol)
@@ -194,9 +216,51 @@ template <> struct V4<float> {
         const float2 u = reinterpret_cast<const float2 *>(p)[0];
         a = u.x; b = u.y;
     }
+    static __device__ __forceinline__ void ldg(const float *p, float &a, float &b, float &c, float &d, uint64_t pol) {
+        asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                     : "=f"(a), "=f"(b), "=f"(c), "=f"(d)
+                     : "l"(p), "l"(pol));
+    }
     static __device__ __forceinline__ void stg(float *p, float a, float b, float c, float d, uint64_t pol) {
         asm volatile("st.global.L1::no_allocate.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(a),
                      "f"(b), "f"(c), "f"(d), "l"(pol)
+                     : "memory");
+    }
+};
+
+// 2-element vector accesses (one 16-byte / 8-byte access per lane, so a
+// warp covers a contiguous span: bank-conflict free in shared memory and
+// fully coalesced in global memory).
+template <typename T> struct V2;
+template <> struct V2<double> {
+    static __device__ __forceinline__ void lds(const double *p, double &a, double &b) {
+        const double2 u = *reinterpret_cast<const double2 *>(p);
+        a = u.x; b = u.y;
+    }
+    static __device__ __forceinline__ void ldg(const double *p, double &a, double &b, uint64_t pol) {
+        asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+                     : "=d"(a), "=d"(b)
+                     : "l"(p), "l"(pol));
+    }
+    static __device__ __forceinline__ void stg(double *p, double a, double b, uint64_t pol) {
+        asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(a), "d"(b),
+                     "l"(pol)
+                     : "memory");
+    }
+};
+template <> struct V2<float> {
+    static __device__ __forceinline__ void lds(const float *p, float &a, float &b) {
+        const float2 u = *reinterpret_cast<const float2 *>(p);
+        a = u.x; b = u.y;
+    }
+    static __device__ __forceinline__ void ldg(const float *p, float &a, float &b, uint64_t pol) {
+        asm volatile("ld.global.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+                     : "=f"(a), "=f"(b)
+                     : "l"(p), "l"(pol));
+    }
+    static __device__ __forceinline__ void stg(float *p, float a, float b, uint64_t pol) {
+        asm volatile("st.global.L1::no_allocate.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(a), "f"(b),
+                     "l"(pol)
                      : "memory");
     }
 };

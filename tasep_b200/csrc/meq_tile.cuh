@@ -40,7 +40,8 @@ constexpr int kTile = 1 << kTileBits;               // states per tile
 constexpr int kConsumerWarps = 16;
 constexpr int kConsumers = kConsumerWarps * 32;      // 512: one group of 4 states each
 constexpr int kTileThreads = kConsumers + 32;        // + producer warp
-constexpr int kRingSlots = 4;
+constexpr int kMaxRing = 16;                       // partner ring slots (upper bound)
+constexpr int kSmemMax = 232448;                   // dynamic shared memory per CTA on sm_100
 static_assert(kTile / 4 == kConsumers, "one group of four states per consumer thread");
 
 struct TileParams {
@@ -104,7 +105,7 @@ template <typename E> struct StageT<ST_U4, E> {
 
 struct TileCtrl {
     uint64_t full[2], empty[2];
-    uint64_t rfull[kRingSlots], rempty[kRingSlots];
+    uint64_t rfull[kMaxRing], rempty[kMaxRing];
     double wsum[kConsumerWarps];
     double rates_d[kMaxR + 1];
     float rates_f[kMaxR + 3];
@@ -122,9 +123,13 @@ template <int S, typename E> struct TileLayout {
     static constexpr int x0b = Tr::NX > 0 ? kTile * sizeof(typename Tr::X0) : 0;
     static constexpr int x1b = Tr::NX > 1 ? kTile * sizeof(typename Tr::X1) : 0;
     static constexpr int x2b = Tr::NX > 2 ? kTile * sizeof(typename Tr::X2) : 0;
-    static constexpr int stage = gb + x0b + x1b + x2b;
+    static constexpr int stage = gb;     // the gathered tile; extras go straight to registers
     static constexpr int dtab = 2 * gb;  // low diagonal prefixes, for top bit clear / set
-    static constexpr int bytes = kCtrlBytes + 2 * stage + kRingSlots * gb + dtab;
+    // as many partner slots as shared memory holds
+    static constexpr int RS0 = (kSmemMax - kCtrlBytes - 2 * stage - dtab) / gb;
+    static constexpr int RS = RS0 < kMaxRing ? RS0 : kMaxRing;
+    static constexpr int bytes = kCtrlBytes + 2 * stage + RS * gb + dtab;
+    static_assert(RS >= 4, "partner ring too shallow");
 };
 
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory"); }
@@ -148,7 +153,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     TileCtrl &c = *reinterpret_cast<TileCtrl *>(tile_smem);
     unsigned char *stage_base = tile_smem + kCtrlBytes;
     unsigned char *ring_base = stage_base + 2 * LY::stage;
-    G *dtab = reinterpret_cast<G *>(ring_base + kRingSlots * LY::gb);
+    G *dtab = reinterpret_cast<G *>(ring_base + LY::RS * LY::gb);
+    constexpr int RS = LY::RS;
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
@@ -162,7 +168,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             mbar_init(&c.full[b], 1);
             mbar_init(&c.empty[b], kConsumerWarps);
         }
-        for (int s = 0; s < kRingSlots; ++s) {
+        for (int s = 0; s < RS; ++s) {
             mbar_init(&c.rfull[s], 1);
             mbar_init(&c.rempty[s], kConsumerWarps);
         }
@@ -183,7 +189,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         // ---------------- producer ----------------
         if (lane == 0) {
             const uint64_t keep = policy_evict_last();
-            const uint64_t once = policy_evict_first();
             uint32_t it = 0, cur = 0;
             bool ok = true;
             for (unsigned long long T = blockIdx.x; T < p.ntiles && ok; T += gridDim.x, ++it) {
@@ -192,14 +197,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 unsigned char *st = stage_base + b * LY::stage;
                 mbar_arrive_expect_tx(&c.full[b], LY::stage);
                 bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], keep);
-                if constexpr (Tr::NX > 0)
-                    bulk_g2s(st + LY::gb, static_cast<const X0 *>(p.s0) + T * kTile, LY::x0b, &c.full[b], once);
-                if constexpr (Tr::NX > 1)
-                    bulk_g2s(st + LY::gb + LY::x0b, static_cast<const X1 *>(p.s1) + T * kTile, LY::x1b,
-                             &c.full[b], once);
-                if constexpr (Tr::NX > 2)
-                    bulk_g2s(st + LY::gb + LY::x0b + LY::x1b, static_cast<const X2 *>(p.s2) + T * kTile,
-                             LY::x2b, &c.full[b], once);
                 // partner tiles, in the order the consumers add them
                 const bool top = (T >> (ntb - 1)) & 1;
                 const bool strad = !(T & 1);
@@ -220,8 +217,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                         hm &= hm - 1;
                         src = T + (1ull << u);
                     }
-                    const int slot = cur % kRingSlots;
-                    if (cur >= kRingSlots && !mbar_wait(&c.rempty[slot], ((cur / kRingSlots) - 1) & 1, errf)) {
+                    const int slot = cur % RS;
+                    if (cur >= RS && !mbar_wait(&c.rempty[slot], ((cur / RS) - 1) & 1, errf)) {
                         ok = false;
                         break;
                     }
@@ -237,8 +234,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                     const uint32_t uses = (it + 1 - b) / 2;  // tiles started on buffer b
                     if (uses) mbar_drain(&c.full[b], (uses - 1) & 1, 100000000ull);
                 }
-                for (int s = 0; s < kRingSlots; ++s) {
-                    const uint32_t uses = cur > uint32_t(s) ? (cur - 1 - s) / kRingSlots + 1 : 0;
+                for (int s = 0; s < RS; ++s) {
+                    const uint32_t uses = cur > uint32_t(s) ? (cur - 1 - s) / RS + 1 : 0;
                     if (uses) mbar_drain(&c.rfull[s], (uses - 1) & 1, 100000000ull);
                 }
             }
@@ -247,6 +244,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     }
 
     // ---------------- consumers ----------------
+    // Thread t owns two pairs of states: P0 = {2t, 2t+1} and P1 = {2t+1024,
+    // 2t+1025} (local indices).  State bit 0 lies inside a pair, bits 1..9 are
+    // t, bit 10 selects the pair.  A warp's 16-byte accesses to a pair array
+    // cover 512 contiguous bytes, so shared-memory reads are conflict free.
+    //
     // Low diagonal prefixes: d = 0; -r[n] if b0; -r[0] if top clear; then
     // -r[n-1-j] for j = 0..9 where b_j = 0, b_(j+1) = 1 (src/lib/solv.c:103-116).
     for (int l = tid; l < kTile; l += kConsumers) {
@@ -259,18 +261,20 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             dtab[tp * kTile + l] = d;
         }
     }
-    const G rn = rate_of<G>(c, n), r0 = rate_of<G>(c, 0), rn1 = rate_of<G>(c, n - 1), rn2 = rate_of<G>(c, n - 2);
-    const G rnL = rate_of<G>(c, n - kTileBits);
-    G rq[kTileBits - 3];  // hop k = q + 2 uses r[n-3-q]
+    const G rn = rate_of<G>(c, n), r0 = rate_of<G>(c, 0), rn1 = rate_of<G>(c, n - 1);
+    const G r9 = rate_of<G>(c, n - 10), rnL = rate_of<G>(c, n - kTileBits);
+    G rq[kTileBits - 3];  // hop k = q + 1 (q = 0..7) uses r[n-2-q]
 #pragma unroll
-    for (int q = 0; q < kTileBits - 3; ++q) rq[q] = rate_of<G>(c, n - 3 - q);
+    for (int q = 0; q < kTileBits - 3; ++q) rq[q] = rate_of<G>(c, n - 2 - q);
     consumer_sync();
 
     const uint64_t once = policy_evict_first();
     O *__restrict__ out = static_cast<O *>(p.out);
-    const uint32_t grp = tid;          // group of 4 states: local states 4*grp .. 4*grp+3
-    const int base = 4 * tid;
-    const bool hi10 = (grp >> 8) & 1;  // state bit 10 (warp-uniform)
+    const uint32_t t9 = tid;              // state bits 1..9
+    const int pb0 = 2 * tid;              // local index of P0
+    const int pb1 = 2 * tid + kTile / 2;  // local index of P1
+    const bool b9 = (t9 >> 8) & 1;        // state bit 9 (warp-uniform)
+    const bool b1clear = !(t9 & 1);       // state bit 1 clear
     double cs = 0.0;
     uint32_t it = 0, cur = 0;
     bool ok = true;
@@ -282,30 +286,54 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         const unsigned long long lowmask = ntb >= 2 ? ((1ull << (ntb - 1)) - 1) : 0ull;
         const unsigned long long hmask = T & ~(T >> 1) & lowmask;
         const unsigned long long dhmask = ~T & (T >> 1) & lowmask;
+        const unsigned long long gT = T * kTile;
 
+        // per-state extra inputs, read once straight into registers; they are
+        // only needed in the epilogue, so their latency hides behind the sweep
+        X0 xa[4];
+        X1 xb[4];
+        X2 xc[4];
+        if constexpr (Tr::NX > 0) {
+            const X0 *s = static_cast<const X0 *>(p.s0) + gT;
+            V2<X0>::ldg(s + pb0, xa[0], xa[1], once);
+            V2<X0>::ldg(s + pb1, xa[2], xa[3], once);
+        }
+        if constexpr (Tr::NX > 1) {
+            const X1 *s = static_cast<const X1 *>(p.s1) + gT;
+            V2<X1>::ldg(s + pb0, xb[0], xb[1], once);
+            V2<X1>::ldg(s + pb1, xb[2], xb[3], once);
+        }
+        if constexpr (Tr::NX > 2) {
+            const X2 *s = static_cast<const X2 *>(p.s2) + gT;
+            V2<X2>::ldg(s + pb0, xc[0], xc[1], once);
+            V2<X2>::ldg(s + pb1, xc[2], xc[3], once);
+        }
         G a0 = G(0), a1 = G(0), a2 = G(0), a3 = G(0);
         int eslot = 0;
         if (top) {  // 1. entry
-            eslot = cur % kRingSlots;
-            if (!mbar_wait(&c.rfull[eslot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
+            eslot = cur % RS;
+            if (!mbar_wait(&c.rfull[eslot], (cur / RS) & 1, errf)) { ok = false; break; }
             const G *ent = reinterpret_cast<const G *>(ring_base + eslot * LY::gb);
             G e0, e1, e2, e3;
-            V4<G>::lds(ent + base, e0, e1, e2, e3);
+            V2<G>::lds(ent + pb0, e0, e1);
+            V2<G>::lds(ent + pb1, e2, e3);
             a0 = A::madd(a0, r0, e0); a1 = A::madd(a1, r0, e1);
             a2 = A::madd(a2, r0, e2); a3 = A::madd(a3, r0, e3);
             ++cur;  // the slot is released after the in-tile terms below
         }
         if (!mbar_wait(&c.full[b], (it >> 1) & 1, errf)) { ok = false; break; }
-        unsigned char *st = stage_base + b * LY::stage;
-        const G *xs = reinterpret_cast<const G *>(st);
+        const G *xs = reinterpret_cast<const G *>(stage_base + b * LY::stage);
 
         G x0, x1, x2, x3;
-        V4<G>::lds(xs + base, x0, x1, x2, x3);
+        V2<G>::lds(xs + pb0, x0, x1);
+        V2<G>::lds(xs + pb1, x2, x3);
         // 2. diagonal: low prefix from the table, then j = 10 and j >= 11
+        const G *dt = dtab + (top ? kTile : 0);
         G d0, d1, d2, d3;
-        V4<G>::lds(dtab + (top ? kTile : 0) + base, d0, d1, d2, d3);
-        if (!hi10 && !strad) {  // j = 10: b10 = 0, b11 = 1
-            d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL); d2 = A::sub(d2, rnL); d3 = A::sub(d3, rnL);
+        V2<G>::lds(dt + pb0, d0, d1);
+        V2<G>::lds(dt + pb1, d2, d3);
+        if (!strad) {  // j = 10: b10 = 0 (P0), b11 = 1
+            d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL);
         }
         {
             unsigned long long mh = dhmask;
@@ -318,42 +346,47 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         }
         a0 = A::madd(a0, d0, x0); a1 = A::madd(a1, d1, x1);
         a2 = A::madd(a2, d2, x2); a3 = A::madd(a3, d3, x3);
-        // 3. exit (b0 clear: states 0 and 2 of the group)
+        // 3. exit (b0 clear: the first state of each pair)
         a0 = A::madd(a0, rn, x1);
         a2 = A::madd(a2, rn, x3);
         // 4. hops, ascending bit
-        a1 = A::madd(a1, rn1, x2);  // k = 0
-        if (!(grp & 1)) {           // k = 1
-            G p0, p1;
-            V4<G>::lds2(xs + base + 4, p0, p1);
-            a2 = A::madd(a2, rn2, p0);
-            a3 = A::madd(a3, rn2, p1);
+        {  // k = 0: second state of a pair with bit 1 clear <- first state of the next pair (next lane)
+            const G n0 = __shfl_down_sync(0xffffffffu, x0, 1);
+            const G n2 = __shfl_down_sync(0xffffffffu, x2, 1);
+            if (b1clear) {
+                a1 = A::madd(a1, rn1, n0);
+                a3 = A::madd(a3, rn1, n2);
+            }
         }
 #pragma unroll
-        for (int q = 0; q < kTileBits - 3; ++q) {  // k = q + 2 = 2..9
-            if (((grp >> q) & 3u) == 1u) {
+        for (int q = 0; q < kTileBits - 3; ++q) {  // k = q + 1 = 1..8: partner pair t + 2^q
+            if (((t9 >> q) & 3u) == 1u) {
+                const int po = 2 << q;
                 G p0, p1, p2, p3;
-                V4<G>::lds(xs + base + (4 << q), p0, p1, p2, p3);
+                V2<G>::lds(xs + pb0 + po, p0, p1);
+                V2<G>::lds(xs + pb1 + po, p2, p3);
                 a0 = A::madd(a0, rq[q], p0); a1 = A::madd(a1, rq[q], p1);
                 a2 = A::madd(a2, rq[q], p2); a3 = A::madd(a3, rq[q], p3);
             }
         }
-        if (top) {
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&c.rempty[eslot]);
+        if (b9) {  // k = 9: P0 states with b9 set <- pair t + 256 (bit 9 clear, bit 10 set)
+            G p0, p1;
+            V2<G>::lds(xs + pb0 + kTile / 4, p0, p1);
+            a0 = A::madd(a0, r9, p0);
+            a1 = A::madd(a1, r9, p1);
         }
-        if (strad) {  // k = 10: upper half of this tile <- lower half of tile T+1
-            const int slot = cur % kRingSlots;
-            if (!mbar_wait(&c.rfull[slot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
-            if (hi10) {
-                const G *hp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
-                G p0, p1, p2, p3;
-                V4<G>::lds(hp + base - kTile / 2, p0, p1, p2, p3);
-                a0 = A::madd(a0, rnL, p0); a1 = A::madd(a1, rnL, p1);
-                a2 = A::madd(a2, rnL, p2); a3 = A::madd(a3, rnL, p3);
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&c.rempty[slot]);
+        if (top) {
+            consumer_release(&c.rempty[eslot], lane);
+        }
+        if (strad) {  // k = 10: P1 <- lower half of tile T+1
+            const int slot = cur % RS;
+            if (!mbar_wait(&c.rfull[slot], (cur / RS) & 1, errf)) { ok = false; break; }
+            const G *hp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
+            G p2, p3;
+            V2<G>::lds(hp + pb0, p2, p3);
+            a2 = A::madd(a2, rnL, p2);
+            a3 = A::madd(a3, rnL, p3);
+            consumer_release(&c.rempty[slot], lane);
             ++cur;
         }
         {
@@ -361,25 +394,22 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             while (mh) {
                 const int u = __ffsll(mh) - 1;
                 mh &= mh - 1;
-                const int slot = cur % kRingSlots;
-                if (!mbar_wait(&c.rfull[slot], (cur / kRingSlots) & 1, errf)) { ok = false; break; }
+                const int slot = cur % RS;
+                if (!mbar_wait(&c.rfull[slot], (cur / RS) & 1, errf)) { ok = false; break; }
                 const G *pp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
                 const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 G p0, p1, p2, p3;
-                V4<G>::lds(pp + base, p0, p1, p2, p3);
+                V2<G>::lds(pp + pb0, p0, p1);
+                V2<G>::lds(pp + pb1, p2, p3);
                 a0 = A::madd(a0, rr, p0); a1 = A::madd(a1, rr, p1);
                 a2 = A::madd(a2, rr, p2); a3 = A::madd(a3, rr, p3);
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&c.rempty[slot]);
+                consumer_release(&c.rempty[slot], lane);
                 ++cur;
             }
             if (!ok) break;
         }
 
         // ---- epilogue ----
-        const X0 *xa = reinterpret_cast<const X0 *>(st + LY::gb);
-        const X1 *xb = reinterpret_cast<const X1 *>(st + LY::gb + LY::x0b);
-        const X2 *xc = reinterpret_cast<const X2 *>(st + LY::gb + LY::x0b + LY::x1b);
         const G acc[4] = {a0, a1, a2, a3};
         const G xv[4] = {x0, x1, x2, x3};
         O o[4];
@@ -399,19 +429,19 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             } else if constexpr (S == ST_H2) {
                 o[j] = static_cast<O>(xv[j] + static_cast<G>(p.hc) * Tv);
             } else if constexpr (S == ST_H3) {
-                o[j] = static_cast<O>(xa[base + j] + static_cast<G>(p.hc) * Tv);
+                o[j] = static_cast<O>(xa[j] + static_cast<G>(p.hc) * Tv);
             } else if constexpr (S == ST_H4) {
-                const double D = static_cast<double>(xa[base + j]) + p.hc * static_cast<double>(Tv);
-                o[j] = xb[base + j] + D;
+                const double D = static_cast<double>(xa[j]) + p.hc * static_cast<double>(Tv);
+                o[j] = xb[j] + D;
                 cs += fabs(D);
             } else if constexpr (S == ST_U1) {
                 o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xv[j]);
             } else if constexpr (S == ST_U2 || S == ST_U3) {
-                o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xa[base + j]);
+                o[j] = __dadd_rn(__dmul_rn(p.hc, Tv), xa[j]);
             } else if constexpr (S == ST_U4) {
-                const double x = xa[base + j];
-                const double k1 = 2.0 * (xb[base + j] - x);
-                const double k2 = 2.0 * (xc[base + j] - x);
+                const double x = xa[j];
+                const double k1 = 2.0 * (xb[j] - x);
+                const double k2 = 2.0 * (xc[j] - x);
                 const double k3 = xv[j] - x;
                 const double k4 = __dmul_rn(p.h, Tv);
                 const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4), 6.0);
@@ -419,9 +449,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 cs += fabs(D);
             }
         }
-        V4<O>::stg(out + T * kTile + base, o[0], o[1], o[2], o[3], once);
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&c.empty[b]);
+        V2<O>::stg(out + gT + pb0, o[0], o[1], once);
+        V2<O>::stg(out + gT + pb1, o[2], o[3], once);
+        consumer_release(&c.empty[b], lane);
     }
     if (!ok || *errf) atomicExch(&p.ex->error, 1);
 

@@ -239,3 +239,44 @@ def test_rk4_steps_many_tiles():
         mass = m.observables()["mass"]
     assert np.max(np.abs(x - xo)) <= PROB_TOL
     assert abs(mass - 1.0) < 1e-13
+
+
+@pytest.mark.parametrize("integrator,precision", [(T.INTEGRATOR_RK4, T.PRECISION_FP64),
+                                                  (T.INTEGRATOR_REF, T.PRECISION_FP64)])
+def test_mass_conservation_n24(integrator, precision):
+    """Generator columns sum to zero, so the total probability stays 1 to rounding
+    (uniform start, 2^24 states, 8192 tiles: every buffer is reused many times)."""
+    n = 24
+    with T.Meq(n, integrator, precision) as m:
+        m.set_rates(rates_for(n, 1))
+        m.init(T.INIT_UNIFORM)
+        m.run(0.01, 23, exit_rule=False)
+        mass = m.observables()["mass"]
+        x = m.store()
+    assert abs(mass - 1.0) < 1e-12
+    assert abs(x.sum() - 1.0) < 1e-12
+
+
+@pytest.mark.parametrize("n,integrator", [(26, O.INT_RK4), (26, O.INT_REF), (28, O.INT_RK4)])
+def test_steps_random_dense_state_full_size(n, integrator):
+    """A random dense state at n=26 and at the benchmark size n=28 (up to 131072
+    tiles, every shared-memory buffer reused hundreds of times per launch): each
+    of two steps within 1e-12 of the oracle for every state (REF: bit-exact)."""
+    r = rates_for(n, 1)
+    x0 = np.random.default_rng(5).random(1 << n)
+    x0 /= x0.sum()
+    xo = x0.copy()
+    with T.Meq(n, integrator) as m:
+        m.set_rates(r)
+        m.load(x0)
+        for _ in range(2):
+            m.run(0.01, 1, exit_rule=False)
+            if integrator == O.INT_RK4:
+                O.step_rk4(n, r, 0.01, xo)
+            else:
+                O.step_ref(n, r, 0.01, xo)
+            y = m.store()
+            if integrator == O.INT_REF:
+                assert np.array_equal(y, xo), _mismatch_report(y, xo)
+            else:
+                assert np.max(np.abs(y - xo)) <= PROB_TOL, _mismatch_report(y, xo)
