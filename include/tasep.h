@@ -170,6 +170,31 @@ tasep_status tasep_apply_device(int n, const double *rates, const double *x, dou
 tasep_status tasep_step_ref_device(int n, const double *rates, double h, const double *x,
                                    double *x_out, double *checksum_host, void *stream);
 
+/* The same reference step as tasep_step_ref_device, for callers that must not
+ * allocate device memory: a host program whose device memory is all handed
+ * out by its own pool allocator (and which forbids plugins from calling
+ * cudaMalloc, since a raw allocation fragments or escapes that pool), or a
+ * loop that cannot afford the device-wide synchronisation cudaMalloc and
+ * cudaFree may cause.  No counterpart in the reference.
+ *
+ * It allocates nothing: the scratch for the L1 norm (one partial sum per CTA,
+ * a ticket counter and the step's status) is a fixed 8.3 KB array in the
+ * library's device image, which every GPU that loads the library holds until
+ * the process exits.  It holds at most 1024 per-CTA partial sums; the step
+ * launches one CTA per SM, and a device with more SMs than that is rejected
+ * with TASEP_ERR_INVALID.  The first call on a device looks up that array's
+ * device address (and the device's SM count); make that first call before any
+ * stream capture.  The caller passes every input and output: x and x_out
+ * (2^n doubles each, device memory, not overlapping), rates (n+1 doubles,
+ * host memory) and checksum_dev (one double in device memory that receives the
+ * step's L1 norm; NULL skips it).  Nothing is synchronised; results are ready
+ * when `stream` reaches them.  All calls share the one array, and each call
+ * clears its counter and status first, so calls that overlap on the GPU (on
+ * different streams or from different threads without ordering) race and
+ * must not be issued. */
+tasep_status tasep_step_ref_device_noalloc(int n, const double *rates, double h, const double *x,
+                                           double *x_out, double *checksum_dev, void *stream);
+
 /* ---- misc ---------------------------------------------------------------- */
 const char *tasep_last_error(void);
 int tasep_abi_version(void);

@@ -33,6 +33,7 @@ EXPORTS = (
     "tasep_meq_enqueue_steps", "tasep_meq_synchronize", "tasep_meq_store", "tasep_meq_observables",
     "tasep_meq_stream", "tasep_meq_profile", "tasep_meq_profile_read", "tasep_apply_device",
     "tasep_step_ref_device", "tasep_last_error", "tasep_abi_version", "tasep_meq_footprint",
+    "tasep_step_ref_device_noalloc",
 )
 
 
@@ -91,6 +92,8 @@ def lib():
                                              C.POINTER(C.c_int)]
         L.tasep_apply_device.argtypes = [C.c_int, _dp, C.c_void_p, C.c_void_p, C.c_void_p]
         L.tasep_step_ref_device.argtypes = [C.c_int, _dp, C.c_double, C.c_void_p, C.c_void_p, _dp, C.c_void_p]
+        L.tasep_step_ref_device_noalloc.argtypes = [C.c_int, _dp, C.c_double, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p]
         L.tasep_last_error.restype = C.c_char_p
         L.tasep_abi_version.restype = C.c_int
         L.tasep_meq_footprint.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
@@ -220,3 +223,11 @@ def step_ref_device(n, rates, h, x_ptr, out_ptr, stream=None):
     cs = C.c_double(0.0)
     _check(lib().tasep_step_ref_device(n, r.ctypes.data_as(_dp), h, x_ptr, out_ptr, C.byref(cs), stream))
     return cs.value
+
+
+def step_ref_device_noalloc(n, rates, h, x_ptr, out_ptr, checksum_ptr=None, stream=None):
+    """One reference step on device pointers using only the library's static
+    scratch (no device allocation); the L1 norm goes to checksum_ptr (device)."""
+    r = _f64(rates)
+    _check(lib().tasep_step_ref_device_noalloc(n, r.ctypes.data_as(_dp), h, x_ptr, out_ptr, checksum_ptr,
+                                               stream))

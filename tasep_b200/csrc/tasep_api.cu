@@ -713,3 +713,89 @@ tasep_status tasep_step_ref_device(int n, const double *rates, double h, const d
 }
 
 }  // extern "C"
+
+// ---- reference step without any device allocation ----------------------------
+// The scratch of the L1 norm lives in this file-scope device array instead of
+// memory from cudaMalloc.  Host code must not pass the array's name to a
+// kernel (on the host it only stands for the symbol); the device address is
+// looked up once per device with cudaGetSymbolAddress.
+namespace {
+constexpr int kNoAllocMaxCtas = 1024;
+struct NoAllocScratch {
+    ExitState ex;       // status and L1 norm of the last step
+    unsigned counter;   // last-CTA ticket
+    unsigned pad[15];
+    double partials[kNoAllocMaxCtas];
+};
+std::mutex g_noalloc_mu;
+NoAllocScratch *g_noalloc_addr[64] = {};
+int g_noalloc_nsm[64] = {};
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+extern "C" tasep_status tasep_step_ref_device_noalloc(int n, const double *rates, double h, const double *x,
+                                                      double *x_out, double *checksum_dev, void *stream) {
+    if (n < 1 || n > TASEP_MAX_N || !rates || !x || !x_out) return fail(TASEP_ERR_INVALID, "bad argument");
+    if (x == x_out) return fail(TASEP_ERR_INVALID, "x and x_out must not overlap");
+    int dev = 0;
+    CU_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(TASEP_ERR_INVALID, "device ordinal %d out of range", dev);
+    NoAllocScratch *sc = nullptr;
+    int nsm = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {  // set-up on the first call on this device
+            void *addr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+            if (e != cudaSuccess || addr == nullptr)
+                return fail(TASEP_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed: %s",
+                            cudaGetErrorString(e));
+            CU_TRY(cudaDeviceGetAttribute(&g_noalloc_nsm[dev], cudaDevAttrMultiProcessorCount, dev));
+            g_noalloc_addr[dev] = static_cast<NoAllocScratch *>(addr);
+        }
+        sc = g_noalloc_addr[dev];
+        nsm = g_noalloc_nsm[dev];
+    }
+    const unsigned long long ntiles = n > kSmallMaxN ? ((1ull << n) >> kTileBits) : 1ull;
+    const int grid = int(std::min<unsigned long long>(ntiles, (unsigned long long)nsm));
+    if (grid > kNoAllocMaxCtas)
+        return fail(TASEP_ERR_INVALID,
+                    "the step needs %d CTAs but the static scratch holds %d per-CTA partial sums", grid,
+                    kNoAllocMaxCtas);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the array keeps the previous call's contents: clear the status and the ticket
+    CU_TRY(cudaMemsetAsync(sc, 0, offsetof(NoAllocScratch, partials), st));
+    tasep_status s;
+    if (n <= kSmallMaxN) {
+        SmallParams sp;
+        memset(&sp, 0, sizeof sp);
+        sp.n = n;
+        sp.mode = SM_RUN;
+        sp.integrator = SI_REF;
+        sp.x_in = x;
+        sp.x_out = x_out;
+        sp.h = h;
+        sp.max_steps = 1;
+        sp.ex = &sc->ex;
+        fill_const_rates(sp.rs, n, rates);
+        s = launch_small<double>(sp, st);
+    } else {
+        TileParams p;
+        memset(&p, 0, sizeof p);
+        p.n = n;
+        p.ntiles = ntiles;
+        p.g = x;
+        p.out = x_out;
+        p.h = h;
+        p.ex = &sc->ex;
+        p.partials = sc->partials;
+        p.counter = &sc->counter;
+        fill_const_rates(p.rs, n, rates);
+        s = launch_tile<ST_REF, double>(p, grid, st);
+    }
+    if (s) return s;
+    if (checksum_dev)
+        CU_TRY(cudaMemcpyAsync(checksum_dev, &sc->ex.last_checksum, sizeof(double), cudaMemcpyDeviceToDevice, st));
+    return TASEP_OK;
+}
