@@ -1,0 +1,54 @@
+/*
+ * me_host.h - host side of the drop-in masterEquation program: option state,
+ * output writers and small utilities.  C99.
+ */
+#ifndef ME_HOST_H
+#define ME_HOST_H
+
+#include <stdint.h>
+#include <stdio.h>
+
+#define ME_MAX_N 33
+
+/* Fatal error with a timestamp on stderr, as err_exit (reference
+ * src/lib/io.c:13-19). */
+void me_err_exit(const char *msg, int code);
+
+/* Reads `count` doubles with fscanf("%lf"); returns 0 on success. */
+int me_read_doubles(const char *path, int count, double *out, const char *sep_fmt);
+
+/* Observables of the final state, everything the writers need. */
+typedef struct {
+    int n;
+    double y[ME_MAX_N];                /* bit-order densities (condense)      */
+    double cov[ME_MAX_N * ME_MAX_N];   /* site order                           */
+    double mul[ME_MAX_N * ME_MAX_N];   /* site order                           */
+    double p4[(ME_MAX_N - 3) * 16];    /* 4-bit window marginals               */
+} me_obs;
+
+/* Probability file: one line per state, site-0-first bit string then
+ * "\t\t%.20g" (reference src/masterEquation.c:1021-1040).  Formatting runs on
+ * `threads` threads; the file is written in index order. */
+int me_write_probs(const char *path, int n, const double *x, int threads);
+
+/* The remaining files of src/masterEquation.c:1042-1539. */
+void me_write_prb_txt(const char *path);
+void me_write_exp_values(const char *o_filename, const me_obs *ob);
+void me_write_cov(const char *path_mat, const char *path_ppm, const me_obs *ob);
+void me_write_mul(const char *path_mat, const char *path_ppm, const me_obs *ob);
+void me_write_windows(const char *o_filename, const me_obs *ob);
+
+/* Window quantities from the 4-bit marginals (src/masterEquation.c:32-143);
+ * offset as in the reference (bits offset..offset+key_size-1 hold the key). */
+double me_win_point(const me_obs *ob, int key, int key_size, int offset);
+double me_win_corr(const me_obs *ob, int key, int offset);
+double me_win_error_guess(const me_obs *ob, int key, int offset);
+double me_win_closure(const me_obs *ob, int key, int offset);
+
+/* Minimal P6 writer (src/lib/graphlib.c:35-62 format). */
+typedef struct {
+    unsigned char r, g, b;
+} me_pixel;
+int me_write_ppm(const char *path, int rx, int ry, const me_pixel *data);
+
+#endif

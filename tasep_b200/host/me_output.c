@@ -1,0 +1,301 @@
+/*
+ * me_output.c - output files of the drop-in masterEquation program.
+ *
+ * File names, line formats and number formats follow the reference's writers
+ * (src/masterEquation.c:1019-1539, src/lib/graphlib.c:35-62) so that scripts
+ * reading the reference's files read these unchanged.  The values come from
+ * the GPU observables (densities, covariance, 4-bit window marginals); only
+ * the probability vector itself is copied to the host.
+ */
+#include "me_host.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+void me_err_exit(const char *msg, int code) {
+    char date[128];
+    time_t t = time(NULL);
+    struct tm *tmv = localtime(&t);
+    if (!tmv || !strftime(date, sizeof date, "%c", tmv)) date[0] = 0;
+    fprintf(stderr, "[%s]:%s\n", date, msg);
+    exit(code);
+}
+
+int me_read_doubles(const char *path, int count, double *out, const char *fmt) {
+    FILE *f = fopen(path, "r");
+    if (!f) return -1;
+    for (int i = 0; i < count; i++)
+        if (fscanf(f, fmt, &out[i]) == EOF) {
+            fclose(f);
+            return -2;
+        }
+    fclose(f);
+    return 0;
+}
+
+/* ---- probabilities --------------------------------------------------------- */
+
+typedef struct {
+    int n;
+    const double *x;
+    uint64_t begin, end;
+    char *buf;
+    size_t len;
+} fmt_job;
+
+static void *fmt_worker(void *arg) {
+    fmt_job *j = (fmt_job *)arg;
+    char *p = j->buf;
+    const int n = j->n;
+    for (uint64_t i = j->begin; i < j->end; i++) {
+        for (int s = 0; s < n; s++) *p++ = ((i >> (n - 1 - s)) & 1) ? '1' : '0';
+        p += sprintf(p, "\t\t%.20g\n", j->x[i]);
+    }
+    j->len = (size_t)(p - j->buf);
+    return NULL;
+}
+
+int me_write_probs(const char *path, int n, const double *x, int threads) {
+    FILE *f = fopen(path, "w");
+    if (!f) return -1;
+    printf("Writing result vector to file '%s'\n", path);
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    const uint64_t dim = (uint64_t)1 << n;
+    const uint64_t block = (uint64_t)1 << 20;
+    const size_t line_max = (size_t)n + 2 + 40;
+    fmt_job jobs[256];
+    pthread_t tids[256];
+    uint64_t per = (block + threads - 1) / threads;
+    for (int t = 0; t < threads; t++) {
+        jobs[t].buf = (char *)malloc(per * line_max);
+        if (!jobs[t].buf) {
+            fclose(f);
+            return -2;
+        }
+    }
+    for (uint64_t b0 = 0; b0 < dim; b0 += block) {
+        const uint64_t b1 = b0 + block < dim ? b0 + block : dim;
+        int used = 0;
+        for (int t = 0; t < threads; t++) {
+            uint64_t s = b0 + (uint64_t)t * per, e = s + per;
+            if (s >= b1) break;
+            if (e > b1) e = b1;
+            jobs[t].n = n;
+            jobs[t].x = x;
+            jobs[t].begin = s;
+            jobs[t].end = e;
+            if (pthread_create(&tids[t], NULL, fmt_worker, &jobs[t]) != 0) fmt_worker(&jobs[t]), tids[t] = 0;
+            used++;
+        }
+        for (int t = 0; t < used; t++) {
+            if (tids[t]) pthread_join(tids[t], NULL);
+            fwrite(jobs[t].buf, 1, jobs[t].len, f);
+        }
+        printf("-->%f%%\r", 100. * (double)b1 / (double)dim);
+    }
+    printf("\n");
+    for (int t = 0; t < threads; t++) free(jobs[t].buf);
+    fclose(f);
+    return 0;
+}
+
+void me_write_prb_txt(const char *path) {
+    /* per-snapshot probabilities; empty without -a (src/masterEquation.c:1047-1062) */
+    FILE *f = fopen(path, "w");
+    if (f) fclose(f);
+    else printf("ERROR: Cant write to %s\n", path);
+}
+
+/* ---- densities ------------------------------------------------------------------ */
+
+void me_write_exp_values(const char *o, const me_obs *ob) {
+    const int n = ob->n;
+    const size_t size = strlen(o) + 20;
+    char *name = (char *)malloc(size);
+    snprintf(name, size, "%s_exp_values_fin.vec", o);
+    FILE *f = fopen(name, "w");
+    if (f) {
+        for (int i = 0; i < n - 1; i++) fprintf(f, "%lf, ", ob->y[n - 1 - i]);
+        fprintf(f, "%lf", ob->y[0]);
+        fclose(f);
+    }
+    snprintf(name, size, "%s_exp_values_fin.dat", o);
+    f = fopen(name, "w");
+    if (f) {
+        for (int i = 0; i < n; i++) fprintf(f, "%d Pos%d %lf\n", i, i, ob->y[n - 1 - i]);
+        fclose(f);
+    }
+    free(name);
+}
+
+/* ---- matrices and heat maps -------------------------------------------------------- */
+
+int me_write_ppm(const char *path, int rx, int ry, const me_pixel *data) {
+    FILE *f = fopen(path, "w");
+    if (!f) return -1;
+    fprintf(f, "P6\n%d %d\n255\n", rx, ry);
+    for (int i = 0; i < rx * ry; i++) fwrite(&data[i], 1, 3, f);
+    fclose(f);
+    return 0;
+}
+
+static void write_matrix(const char *path, int n, const double *m) {
+    FILE *f = fopen(path, "w");
+    if (!f) return;
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < n; k++) fprintf(f, k < n - 1 ? "%lf, " : "%lf\n", m[i * n + k]);
+    fclose(f);
+}
+
+/* Colour of one covariance entry (src/masterEquation.c:1163-1190): blue for
+ * negative, red for positive, green near zero; 255*|c|^(1/4) converted to
+ * int, then stored in a byte. */
+static me_pixel cov_colour(double c) {
+    const double intensity = 0.25;
+    int r, g, b;
+    if (c < 0 && fabs(c) > 0.0001) {
+        r = 0;
+        g = 0;
+        b = (-1) * pow(fabs(c), intensity) * 255;
+    } else if (c > 0 && fabs(c) > 0.0001) {
+        r = pow(c, intensity) * 255;
+        g = 0;
+        b = 0;
+    } else {
+        r = 0;
+        g = fabs(pow(fabs(c), intensity) * 255);
+        b = 0;
+    }
+    me_pixel p = {(unsigned char)r, (unsigned char)g, (unsigned char)b};
+    return p;
+}
+
+/* Grey level of one product entry (src/masterEquation.c:1331-1341). */
+static me_pixel mul_colour(double m) {
+    const double intensity = 0.25;
+    int v = (-1) * pow(fabs(m), intensity) * 255;
+    me_pixel p = {(unsigned char)v, (unsigned char)v, (unsigned char)v};
+    return p;
+}
+
+/* Pixel (x = i, y = k) shows matrix entry [i][k] (set_pixel, src/lib/graphlib.c:86-98). */
+static void write_map(const char *path, int n, const double *m, me_pixel (*colour)(double)) {
+    me_pixel *img = (me_pixel *)malloc(sizeof(me_pixel) * (size_t)n * (size_t)n);
+    if (!img) return;
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < n; k++) img[k * n + i] = colour(m[i * n + k]);
+    me_write_ppm(path, n, n, img);
+    free(img);
+}
+
+void me_write_cov(const char *path_mat, const char *path_ppm, const me_obs *ob) {
+    write_matrix(path_mat, ob->n, ob->cov);
+    write_map(path_ppm, ob->n, ob->cov, cov_colour);
+}
+
+void me_write_mul(const char *path_mat, const char *path_ppm, const me_obs *ob) {
+    write_matrix(path_mat, ob->n, ob->mul);
+    write_map(path_ppm, ob->n, ob->mul, mul_colour);
+}
+
+/* ---- window observables ----------------------------------------------------------- */
+
+/* Sum of probabilities of the states whose bits offset..offset+key_size-1
+ * equal key (key_fit, src/masterEquation.c:32-45), from the marginals of the
+ * 4-bit window that contains those bits. */
+double me_win_point(const me_obs *ob, int key, int key_size, int offset) {
+    int p = offset < ob->n - 4 ? offset : ob->n - 4;
+    if (p < 0) return 0.0;
+    const int sh = offset - p, mask = (1 << key_size) - 1;
+    double s = 0.0;
+    for (int q = 0; q < 16; q++)
+        if (((q >> sh) & mask) == key) s += ob->p4[p * 16 + q];
+    return s;
+}
+
+static void win_terms(const me_obs *ob, int key, int offset, double *lr, double *no, double *le, double *re) {
+    const int key_size = 2;
+    *lr = me_win_point(ob, (key << 1) + 1 + (1 << (key_size + 1)), key_size + 2, offset - 1);
+    *no = me_win_point(ob, key, key_size, offset);
+    *le = me_win_point(ob, key + (1 << key_size), key_size + 1, offset);
+    *re = me_win_point(ob, (key << 1) + 1, key_size + 1, offset - 1);
+}
+
+/* high_order_corr (src/masterEquation.c:47-75): the correlation coefficient it
+ * computes.  The reference function returns nothing (undefined behaviour). */
+double me_win_corr(const me_obs *ob, int key, int offset) {
+    double lr, no, le, re;
+    win_terms(ob, key, offset, &lr, &no, &le, &re);
+    return (lr * no - le * re) / sqrt(le * (no - le) * re * (no - re));
+}
+
+/* error_guess (src/masterEquation.c:77-101). */
+double me_win_error_guess(const me_obs *ob, int key, int offset) {
+    double lr, no, le, re;
+    win_terms(ob, key, offset, &lr, &no, &le, &re);
+    return (lr / no - (le / no) * (re / no)) * no;
+}
+
+/* higher_order_pf_approx (src/masterEquation.c:103-127): P(L)P(R)/P(middle). */
+double me_win_closure(const me_obs *ob, int key, int offset) {
+    double lr, no, le, re;
+    win_terms(ob, key, offset, &lr, &no, &le, &re);
+    return (le * re) / no;
+}
+
+void me_write_windows(const char *o, const me_obs *ob) {
+    const int n = ob->n;
+    int mask_size = 2;
+    const size_t size = strlen(o) + 24;
+    char *name = (char *)malloc(size);
+    FILE *f;
+
+    printf("Calculating Higher Order Correlations\n");
+    snprintf(name, size, "%s_highcorr", o);
+    if ((f = fopen(name, "w")) != NULL) {
+        for (int i = 1; i < n - mask_size; i++) fprintf(f, "\t\t\t%d", i);
+        fprintf(f, "\n");
+        for (int key = 0; key < (1 << mask_size); key++) {
+            for (int i = 0; i < mask_size; i++) fprintf(f, (key >> (mask_size - 1 - i)) & 1 ? "1" : "0");
+            fprintf(f, "\t");
+            for (int i = 1; i < n - mask_size; i++) fprintf(f, "%1.4g\t", me_win_corr(ob, key, n - mask_size - i));
+            fprintf(f, "\n");
+        }
+        fclose(f);
+    }
+
+    const int mask = (1 << mask_size) - 1;
+    printf("Calculating error guess\n");
+    snprintf(name, size, "%s_error_guess", o);
+    if ((f = fopen(name, "w")) != NULL) {
+        for (int i = 1; i < n - mask_size; i++)
+            fprintf(f, "Error guess for t_%d...t_%d:\t %lf\n", i - 1, i + mask_size,
+                    me_win_error_guess(ob, mask, n - mask_size - i));
+        fclose(f);
+    }
+
+    printf("Calculating closures\n");
+    snprintf(name, size, "%s_closures", o);
+    if ((f = fopen(name, "w")) != NULL) {
+        for (int i = 1; i < n - mask_size; i++)
+            fprintf(f, "Value for closure of t_%d...t_%d:\t %lf\n", i - 1, i + mask_size,
+                    me_win_closure(ob, mask, n - mask_size - i));
+        fclose(f);
+    }
+
+    /* the reference sizes this name one character short twice over
+       (src/masterEquation.c:1499-1501): the file is "..._high_order_point_fun" */
+    mask_size += 2;
+    snprintf(name, size, "%s_high_order_point_fun", o);
+    if ((f = fopen(name, "w")) != NULL) {
+        for (int i = 0; i < n - mask_size + 1; i++)
+            fprintf(f, "t_%d...t_%d = %lf\n", i, mask_size + i - 1,
+                    me_win_point(ob, (1 << mask_size) - 1, mask_size, n - mask_size - i));
+        fclose(f);
+    }
+    free(name);
+}
