@@ -263,9 +263,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     }
     const G rn = rate_of<G>(c, n), r0 = rate_of<G>(c, 0), rn1 = rate_of<G>(c, n - 1);
     const G r9 = rate_of<G>(c, n - 10), rnL = rate_of<G>(c, n - kTileBits);
-    G rq[kTileBits - 3];  // hop k = q + 1 (q = 0..7) uses r[n-2-q]
-#pragma unroll
-    for (int q = 0; q < kTileBits - 3; ++q) rq[q] = rate_of<G>(c, n - 2 - q);
     consumer_sync();
 
     const uint64_t once = policy_evict_first();
@@ -275,8 +272,27 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     const int pb1 = 2 * tid + kTile / 2;  // local index of P1
     const bool b9 = (t9 >> 8) & 1;        // state bit 9 (warp-uniform)
     const bool b1clear = !(t9 & 1);       // state bit 1 clear
+    // In-tile hops k = q+1 (q = 0..7) need t bit q set and bit q+1 clear: a
+    // per-thread constant.  At most 4 such q; keep their partner offsets and
+    // rates in registers, in ascending q (the reference's order).
+    int qcnt = 0;
+    int qoff[4];
+    G qrate[4];
+    {
+        uint32_t hq = t9 & ~(t9 >> 1) & 0xFFu;
+        qcnt = __popc(hq);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int q = hq ? __ffs(hq) - 1 : 0;
+            hq &= hq - 1;
+            qoff[k] = 2 << q;
+            qrate[k] = rate_of<G>(c, n - 2 - q);
+        }
+    }
     double cs = 0.0;
-    uint32_t it = 0, cur = 0;
+    uint32_t it = 0;
+    int cslot = 0;     // next ring slot to consume
+    uint32_t cph = 0;  // its fill parity
     bool ok = true;
 
     for (unsigned long long T = blockIdx.x; T < p.ntiles; T += gridDim.x, ++it) {
@@ -311,15 +327,15 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         G a0 = G(0), a1 = G(0), a2 = G(0), a3 = G(0);
         int eslot = 0;
         if (top) {  // 1. entry
-            eslot = cur % RS;
-            if (!mbar_wait(&c.rfull[eslot], (cur / RS) & 1, errf)) { ok = false; break; }
+            eslot = cslot;
+            if (!mbar_wait(&c.rfull[eslot], cph, errf)) { ok = false; break; }
             const G *ent = reinterpret_cast<const G *>(ring_base + eslot * LY::gb);
             G e0, e1, e2, e3;
             V2<G>::lds(ent + pb0, e0, e1);
             V2<G>::lds(ent + pb1, e2, e3);
             a0 = A::madd(a0, r0, e0); a1 = A::madd(a1, r0, e1);
             a2 = A::madd(a2, r0, e2); a3 = A::madd(a3, r0, e3);
-            ++cur;  // the slot is released after the in-tile terms below
+            if (++cslot == RS) { cslot = 0; cph ^= 1; }  // released after the in-tile terms below
         }
         if (!mbar_wait(&c.full[b], (it >> 1) & 1, errf)) { ok = false; break; }
         const G *xs = reinterpret_cast<const G *>(stage_base + b * LY::stage);
@@ -335,7 +351,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         if (!strad) {  // j = 10: b10 = 0 (P0), b11 = 1
             d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL);
         }
-        {
+        if constexpr (Tr::EXACT) {  // the reference's subtraction order
             unsigned long long mh = dhmask;
             while (mh) {
                 const int u = __ffsll(mh) - 1;
@@ -343,6 +359,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 d0 = A::sub(d0, rr); d1 = A::sub(d1, rr); d2 = A::sub(d2, rr); d3 = A::sub(d3, rr);
             }
+        } else {  // reassociation allowed: one sum of the tile-level rates
+            G ds = G(0);
+            for (unsigned long long mh = dhmask; mh; mh &= mh - 1)
+                ds += rate_of<G>(c, n - 1 - kTileBits - (__ffsll(mh) - 1));
+            d0 -= ds; d1 -= ds; d2 -= ds; d3 -= ds;
         }
         a0 = A::madd(a0, d0, x0); a1 = A::madd(a1, d1, x1);
         a2 = A::madd(a2, d2, x2); a3 = A::madd(a3, d3, x3);
@@ -358,16 +379,27 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 a3 = A::madd(a3, rn1, n2);
             }
         }
+        // k = 1..8: partner pair t + 2^q for this thread's active q (ascending).
+        // Stages that may reassociate collect them in a second accumulator so
+        // the two dependency chains interleave.
+        G c0 = G(0), c1 = G(0), c2 = G(0), c3 = G(0);
 #pragma unroll
-        for (int q = 0; q < kTileBits - 3; ++q) {  // k = q + 1 = 1..8: partner pair t + 2^q
-            if (((t9 >> q) & 3u) == 1u) {
-                const int po = 2 << q;
+        for (int k = 0; k < 4; ++k) {
+            if (k < qcnt) {
                 G p0, p1, p2, p3;
-                V2<G>::lds(xs + pb0 + po, p0, p1);
-                V2<G>::lds(xs + pb1 + po, p2, p3);
-                a0 = A::madd(a0, rq[q], p0); a1 = A::madd(a1, rq[q], p1);
-                a2 = A::madd(a2, rq[q], p2); a3 = A::madd(a3, rq[q], p3);
+                V2<G>::lds(xs + pb0 + qoff[k], p0, p1);
+                V2<G>::lds(xs + pb1 + qoff[k], p2, p3);
+                if constexpr (Tr::EXACT) {
+                    a0 = A::madd(a0, qrate[k], p0); a1 = A::madd(a1, qrate[k], p1);
+                    a2 = A::madd(a2, qrate[k], p2); a3 = A::madd(a3, qrate[k], p3);
+                } else {
+                    c0 = A::madd(c0, qrate[k], p0); c1 = A::madd(c1, qrate[k], p1);
+                    c2 = A::madd(c2, qrate[k], p2); c3 = A::madd(c3, qrate[k], p3);
+                }
             }
+        }
+        if constexpr (!Tr::EXACT) {
+            a0 += c0; a1 += c1; a2 += c2; a3 += c3;
         }
         if (b9) {  // k = 9: P0 states with b9 set <- pair t + 256 (bit 9 clear, bit 10 set)
             G p0, p1;
@@ -379,23 +411,23 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             consumer_release(&c.rempty[eslot], lane);
         }
         if (strad) {  // k = 10: P1 <- lower half of tile T+1
-            const int slot = cur % RS;
-            if (!mbar_wait(&c.rfull[slot], (cur / RS) & 1, errf)) { ok = false; break; }
+            const int slot = cslot;
+            if (!mbar_wait(&c.rfull[slot], cph, errf)) { ok = false; break; }
             const G *hp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
             G p2, p3;
             V2<G>::lds(hp + pb0, p2, p3);
             a2 = A::madd(a2, rnL, p2);
             a3 = A::madd(a3, rnL, p3);
             consumer_release(&c.rempty[slot], lane);
-            ++cur;
+            if (++cslot == RS) { cslot = 0; cph ^= 1; }
         }
         {
             unsigned long long mh = hmask;  // k >= 11
             while (mh) {
                 const int u = __ffsll(mh) - 1;
                 mh &= mh - 1;
-                const int slot = cur % RS;
-                if (!mbar_wait(&c.rfull[slot], (cur / RS) & 1, errf)) { ok = false; break; }
+                const int slot = cslot;
+                if (!mbar_wait(&c.rfull[slot], cph, errf)) { ok = false; break; }
                 const G *pp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
                 const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 G p0, p1, p2, p3;
@@ -404,7 +436,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 a0 = A::madd(a0, rr, p0); a1 = A::madd(a1, rr, p1);
                 a2 = A::madd(a2, rr, p2); a3 = A::madd(a3, rr, p3);
                 consumer_release(&c.rempty[slot], lane);
-                ++cur;
+                if (++cslot == RS) { cslot = 0; cph ^= 1; }
             }
             if (!ok) break;
         }
