@@ -152,6 +152,31 @@ tasep_status tasep_meq_profile(tasep_meq *m, int enable);
 tasep_status tasep_meq_profile_read(tasep_meq *m, const char **names, double *ms,
                                     uint64_t *launches, int cap, int *count);
 
+/* ---- batched parameter sweeps --------------------------------------------
+ * nsys independent systems of the same length n (kTileBits < n <= 24), each
+ * with its own n+1 rates, integrated with classical RK4 (Horner form; FP64 or
+ * MIXED) until each meets the exit rule on its own.  The reference has no
+ * batching; this replaces running bin/masterEquation once per rate vector.
+ * Converged systems retire: later steps skip them.  Steps run as replays of a
+ * CUDA graph of a few steps; the sweep schedule (tiles interleaved over the
+ * SMs, or whole systems per SM) is chosen by timing both. */
+typedef struct tasep_batch tasep_batch;
+tasep_status tasep_batch_create(int n, int nsys, int precision, int device, void *stream, tasep_batch **out);
+tasep_status tasep_batch_destroy(tasep_batch *b);
+/* rates: nsys*(n+1) doubles, system-major. */
+tasep_status tasep_batch_set_rates(tasep_batch *b, const double *rates);
+tasep_status tasep_batch_init(tasep_batch *b, int kind);
+/* host_x: nsys*2^n doubles. */
+tasep_status tasep_batch_load(tasep_batch *b, const double *host_x);
+/* res: nsys results (NULL skips them).  schedule: -1 = choose by timing,
+ * 0 = interleaved, 1 = system per SM; *schedule_used (may be NULL) reports
+ * the choice. */
+tasep_status tasep_batch_run(tasep_batch *b, const tasep_run_config *rc, int schedule, tasep_run_result *res,
+                             int *schedule_used);
+tasep_status tasep_batch_store(const tasep_batch *b, int sys, double *host_x);
+/* Per-bit densities of every system: nsys*n doubles (bit order). */
+tasep_status tasep_batch_densities(tasep_batch *b, double *rho);
+
 /* ---- device-pointer operators ------------------------------------------
  * For callers that keep their own device vectors.  x, y: 2^n doubles in
  * device memory; rates: n+1 doubles in host memory; stream may be NULL. */

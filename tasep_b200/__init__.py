@@ -33,7 +33,8 @@ EXPORTS = (
     "tasep_meq_enqueue_steps", "tasep_meq_synchronize", "tasep_meq_store", "tasep_meq_observables",
     "tasep_meq_stream", "tasep_meq_profile", "tasep_meq_profile_read", "tasep_apply_device",
     "tasep_step_ref_device", "tasep_last_error", "tasep_abi_version", "tasep_meq_footprint",
-    "tasep_step_ref_device_noalloc",
+    "tasep_step_ref_device_noalloc", "tasep_batch_create", "tasep_batch_destroy", "tasep_batch_set_rates",
+    "tasep_batch_init", "tasep_batch_load", "tasep_batch_run", "tasep_batch_store", "tasep_batch_densities",
 )
 
 
@@ -209,6 +210,72 @@ class Meq:
         k = C.c_int(0)
         _check(lib().tasep_meq_profile_read(self._h, names, ms.ctypes.data_as(_dp), cnt, cap, C.byref(k)))
         return {names[i].decode(): (float(ms[i]), int(cnt[i])) for i in range(min(k.value, cap))}
+
+
+class Batch:
+    """nsys independent systems of length n in one sweep (tasep_batch_* calls)."""
+
+    def __init__(self, n, nsys, precision=PRECISION_FP64, device=-1, stream=None):
+        L = lib()
+        H = C.c_void_p
+        if not getattr(L, "_batch_types", False):
+            L.tasep_batch_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.POINTER(H)]
+            L.tasep_batch_destroy.argtypes = [H]
+            L.tasep_batch_set_rates.argtypes = [H, _dp]
+            L.tasep_batch_init.argtypes = [H, C.c_int]
+            L.tasep_batch_load.argtypes = [H, _dp]
+            L.tasep_batch_run.argtypes = [H, C.POINTER(_RunCfg), C.c_int, C.POINTER(RunResult), C.POINTER(C.c_int)]
+            L.tasep_batch_store.argtypes = [H, C.c_int, _dp]
+            L.tasep_batch_densities.argtypes = [H, _dp]
+            L._batch_types = True
+        self.n, self.nsys = n, nsys
+        self._h = H()
+        _check(L.tasep_batch_create(n, nsys, precision, device, stream, C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().tasep_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_rates(self, rates):
+        r = _f64(rates).reshape(self.nsys, self.n + 1)
+        _check(lib().tasep_batch_set_rates(self._h, r.ctypes.data_as(_dp)))
+
+    def init(self, kind=INIT_EMPTY):
+        _check(lib().tasep_batch_init(self._h, kind))
+
+    def load(self, x):
+        x = _f64(x).reshape(self.nsys, 1 << self.n)
+        _check(lib().tasep_batch_load(self._h, x.ctypes.data_as(_dp)))
+
+    def run(self, h, steps, stop_tol=1e-10, stop_count=100, exit_rule=True, schedule=-1, t0=0.0):
+        rc = _RunCfg(t0, h, steps, stop_tol, stop_count, int(bool(exit_rule)))
+        res = (RunResult * self.nsys)()
+        used = C.c_int(-1)
+        _check(lib().tasep_batch_run(self._h, C.byref(rc), schedule, res, C.byref(used)))
+        return [r.as_dict() for r in res], used.value
+
+    def store(self, sys):
+        out = np.empty(1 << self.n)
+        _check(lib().tasep_batch_store(self._h, sys, out.ctypes.data_as(_dp)))
+        return out
+
+    def densities(self):
+        rho = np.empty((self.nsys, self.n))
+        _check(lib().tasep_batch_densities(self._h, rho.ctypes.data_as(_dp)))
+        return rho
 
 
 def apply_device(n, rates, x_ptr, y_ptr, stream=None):

@@ -188,7 +188,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     if (warp == kConsumerWarps) {
         // ---------------- producer ----------------
         if (lane == 0) {
-            const uint64_t keep = policy_evict_last();
+            const uint64_t keep = policy_evict_last();    // partner tiles: read again as self soon
+            const uint64_t normal = policy_evict_normal();
             uint32_t it = 0, cur = 0;
             bool ok = true;
             for (unsigned long long T = blockIdx.x; T < p.ntiles && ok; T += gridDim.x, ++it) {
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 if (it >= 2 && !mbar_wait(&c.empty[b], ((it >> 1) - 1) & 1, errf)) break;
                 unsigned char *st = stage_base + b * LY::stage;
                 mbar_arrive_expect_tx(&c.full[b], LY::stage);
-                bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], keep);
+                bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], normal);  // read again only as a far partner
                 // partner tiles, in the order the consumers add them
                 const bool top = (T >> (ntb - 1)) & 1;
                 const bool strad = !(T & 1);

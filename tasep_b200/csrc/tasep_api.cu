@@ -799,3 +799,5 @@ extern "C" tasep_status tasep_step_ref_device_noalloc(int n, const double *rates
         CU_TRY(cudaMemcpyAsync(checksum_dev, &sc->ex.last_checksum, sizeof(double), cudaMemcpyDeviceToDevice, st));
     return TASEP_OK;
 }
+
+#include "tasep_batch_impl.cuh"

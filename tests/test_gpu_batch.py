@@ -1,0 +1,73 @@
+"""Batched parameter sweeps (tasep_batch_*) against the single-system oracle.
+
+Each system of a batch must end where the oracle's classical RK4 from the
+same rates ends: probabilities within 1e-12 for a fixed number of steps, and,
+under the exit rule, the same exit step (within the rounding-level slack the
+single-system tests allow) and the steady state within 1e-12.  Both sweep
+schedules are exercised, as is retirement: systems that converge early stop
+changing while the rest continue.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import tasep_b200 as T
+
+pytestmark = pytest.mark.gpu
+
+
+def sweep_rates(n, nsys, seed):
+    rng = np.random.default_rng(seed)
+    ab = rng.uniform(0.2, 1.5, (nsys, 2))
+    hops = rng.uniform(0.5, 1.5, (nsys, n - 1))
+    return np.column_stack([ab[:, 0], hops, ab[:, 1]])
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_batch_fixed_steps_matches_oracle(schedule):
+    n, nsys, steps = 13, 5, 300
+    R = sweep_rates(n, nsys, 1)
+    with T.Batch(n, nsys) as b:
+        b.set_rates(R)
+        b.init(T.INIT_EMPTY)
+        res, used = b.run(0.01, steps, exit_rule=False, schedule=schedule)
+        assert used == schedule
+        for s in range(nsys):
+            xo, _ = O.run(n, R[s], h=0.01, steps=steps, integrator=O.INT_RK4, init=O.INIT_EMPTY, exit_rule=False)
+            assert res[s]["steps_done"] == steps
+            assert np.max(np.abs(b.store(s) - xo)) <= 1e-12
+
+
+def test_batch_each_system_to_its_own_steady_state():
+    n, nsys = 12, 8
+    R = sweep_rates(n, nsys, 2)
+    R[0, 0] = R[0, -1] = 1.5   # fast
+    R[1, 0] = R[1, -1] = 0.25  # slow
+    with T.Batch(n, nsys) as b:
+        b.set_rates(R)
+        b.init(T.INIT_EMPTY)
+        res, used = b.run(0.01, 400000, stop_tol=1e-10)
+        rho = b.densities()
+        finals = [b.store(s) for s in range(nsys)]
+    steps = [r["steps_done"] for r in res]
+    assert all(r["converged"] == 1 for r in res)
+    assert steps[1] > steps[0]  # systems retire at different steps
+    for s in range(nsys):
+        xo, ro = O.run(n, R[s], h=0.01, steps=400000, integrator=O.INT_RK4, init=O.INIT_EMPTY, stop_tol=1e-10)
+        assert abs(int(res[s]["steps_done"]) - int(ro["steps_done"])) <= 2
+        assert np.max(np.abs(finals[s] - xo)) <= 1e-12
+        assert np.allclose(rho[s], O.densities(n, xo), rtol=1e-12, atol=0)
+
+
+def test_batch_mixed_precision_densities():
+    n, nsys = 13, 4
+    R = sweep_rates(n, nsys, 3)
+    with T.Batch(n, nsys, T.PRECISION_MIXED) as b:
+        b.set_rates(R)
+        b.init(T.INIT_EMPTY)
+        res, _ = b.run(0.01, 400000, stop_tol=1e-10)
+        rho = b.densities()
+    assert all(r["converged"] == 1 for r in res)
+    for s in range(nsys):
+        xo, _ = O.run(n, R[s], h=0.01, steps=400000, integrator=O.INT_RK4, init=O.INIT_EMPTY, stop_tol=1e-10)
+        assert np.max(np.abs(rho[s] - O.densities(n, xo))) <= 1e-6
