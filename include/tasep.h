@@ -177,6 +177,38 @@ tasep_status tasep_batch_store(const tasep_batch *b, int sys, double *host_x);
 /* Per-bit densities of every system: nsys*n doubles (bit order). */
 tasep_status tasep_batch_densities(tasep_batch *b, double *rho);
 
+/* ---- learned warm start ------------------------------------------------------
+ * No counterpart in the reference.  A per-site network (TASEP_MLP_IN inputs,
+ * three hidden layers of 64 tanh units, 2 outputs: density and nearest-
+ * neighbour covariance) trained on the GPU with the library's own forward,
+ * backward and Adam kernels (BF16 weights, FP32 accumulation), and a device-
+ * side builder of the pair-Markov initial measure from predicted profiles. */
+#define TASEP_MLP_IN 16
+#define TASEP_MLP_OUT 2
+#define TASEP_MLP_PARAMS 9538
+typedef struct tasep_mlp tasep_mlp;
+/* Weights initialised (Glorot-uniform) from `seed`. */
+tasep_status tasep_mlp_create(int device, uint64_t seed, tasep_mlp **out);
+tasep_status tasep_mlp_destroy(tasep_mlp *m);
+tasep_status tasep_mlp_set_params(tasep_mlp *m, const float *params);
+tasep_status tasep_mlp_get_params(tasep_mlp *m, float *params);
+/* Loss sum_s sum_o w[o]*(y_so - t_so)^2 / n and its gradient (host buffers;
+ * x: n*TASEP_MLP_IN, t: n*TASEP_MLP_OUT). */
+tasep_status tasep_mlp_loss_grad(tasep_mlp *m, const float *x, const float *t, int n, const float *out_weights,
+                                 float *loss, float *grad);
+/* Mini-batch Adam on (x, t); loss_per_epoch (may be NULL) gets the mean
+ * training loss of each epoch.  The sample order is shuffled from `seed`. */
+tasep_status tasep_mlp_train(tasep_mlp *m, const float *x, const float *t, int n, const float *out_weights,
+                             int epochs, int batch, float lr, uint64_t seed, float *loss_per_epoch);
+tasep_status tasep_mlp_predict(tasep_mlp *m, const float *x, int n, float *y);
+/* Initial state P(tau) = P(tau_0) prod_j P(tau_(j+1)|tau_j) from densities
+ * rho[j] (site order, n values) and nearest-neighbour covariances cov[j] =
+ * <tau_j tau_(j+1)> - rho_j rho_(j+1) (n-1 values).  Covariances are clipped to
+ * the range a joint distribution allows; a density outside (0,1) returns
+ * TASEP_ERR_INVALID and leaves the state unchanged (the caller falls back to
+ * the empty lattice). */
+tasep_status tasep_meq_init_pair_markov(tasep_meq *m, const double *rho, const double *cov);
+
 /* ---- device-pointer operators ------------------------------------------
  * For callers that keep their own device vectors.  x, y: 2^n doubles in
  * device memory; rates: n+1 doubles in host memory; stream may be NULL. */

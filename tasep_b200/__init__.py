@@ -35,6 +35,8 @@ EXPORTS = (
     "tasep_step_ref_device", "tasep_last_error", "tasep_abi_version", "tasep_meq_footprint",
     "tasep_step_ref_device_noalloc", "tasep_batch_create", "tasep_batch_destroy", "tasep_batch_set_rates",
     "tasep_batch_init", "tasep_batch_load", "tasep_batch_run", "tasep_batch_store", "tasep_batch_densities",
+    "tasep_mlp_create", "tasep_mlp_destroy", "tasep_mlp_set_params", "tasep_mlp_get_params", "tasep_mlp_loss_grad",
+    "tasep_mlp_train", "tasep_mlp_predict", "tasep_meq_init_pair_markov",
 )
 
 
@@ -276,6 +278,86 @@ class Batch:
         rho = np.empty((self.nsys, self.n))
         _check(lib().tasep_batch_densities(self._h, rho.ctypes.data_as(_dp)))
         return rho
+
+
+MLP_IN, MLP_OUT, MLP_PARAMS = 16, 2, 9538
+_fp = C.POINTER(C.c_float)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Mlp:
+    """The per-site surrogate network, trained and evaluated on the GPU."""
+
+    def __init__(self, seed=0, device=-1):
+        L = lib()
+        H = C.c_void_p
+        if not getattr(L, "_mlp_types", False):
+            L.tasep_mlp_create.argtypes = [C.c_int, C.c_uint64, C.POINTER(H)]
+            L.tasep_mlp_destroy.argtypes = [H]
+            L.tasep_mlp_set_params.argtypes = [H, _fp]
+            L.tasep_mlp_get_params.argtypes = [H, _fp]
+            L.tasep_mlp_loss_grad.argtypes = [H, _fp, _fp, C.c_int, _fp, _fp, _fp]
+            L.tasep_mlp_train.argtypes = [H, _fp, _fp, C.c_int, _fp, C.c_int, C.c_int, C.c_float, C.c_uint64, _fp]
+            L.tasep_mlp_predict.argtypes = [H, _fp, C.c_int, _fp]
+            L.tasep_meq_init_pair_markov.argtypes = [H, _dp, _dp]
+            L._mlp_types = True
+        self._h = H()
+        _check(L.tasep_mlp_create(device, seed, C.byref(self._h)))
+
+    def close(self):
+        if self._h:
+            lib().tasep_mlp_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self):
+        p = np.empty(MLP_PARAMS, dtype=np.float32)
+        _check(lib().tasep_mlp_get_params(self._h, p.ctypes.data_as(_fp)))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = _f32(p)
+        assert p.shape == (MLP_PARAMS,)
+        _check(lib().tasep_mlp_set_params(self._h, p.ctypes.data_as(_fp)))
+
+    def loss_grad(self, x, t, out_weights=(1.0, 1.0)):
+        x, t, w = _f32(x), _f32(t), _f32(out_weights)
+        loss = np.zeros(1, dtype=np.float32)
+        g = np.empty(MLP_PARAMS, dtype=np.float32)
+        _check(lib().tasep_mlp_loss_grad(self._h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), len(x),
+                                         w.ctypes.data_as(_fp), loss.ctypes.data_as(_fp), g.ctypes.data_as(_fp)))
+        return float(loss[0]), g
+
+    def train(self, x, t, out_weights=(1.0, 1.0), epochs=100, batch=1024, lr=1e-3, seed=0):
+        x, t, w = _f32(x), _f32(t), _f32(out_weights)
+        losses = np.zeros(max(epochs, 1), dtype=np.float32)
+        _check(lib().tasep_mlp_train(self._h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), len(x),
+                                     w.ctypes.data_as(_fp), epochs, batch, lr, seed, losses.ctypes.data_as(_fp)))
+        return losses[:epochs]
+
+    def predict(self, x):
+        x = _f32(x)
+        y = np.empty((len(x), MLP_OUT), dtype=np.float32)
+        _check(lib().tasep_mlp_predict(self._h, x.ctypes.data_as(_fp), len(x), y.ctypes.data_as(_fp)))
+        return y
+
+
+def init_pair_markov(meq, rho, cov):
+    """Pair-Markov initial measure on a Meq handle; raises TasepError if infeasible."""
+    L = lib()
+    L.tasep_meq_init_pair_markov.argtypes = [C.c_void_p, _dp, _dp]
+    r, c = _f64(rho), _f64(cov)
+    _check(L.tasep_meq_init_pair_markov(meq._h, r.ctypes.data_as(_dp), c.ctypes.data_as(_dp)))
 
 
 def apply_device(n, rates, x_ptr, y_ptr, stream=None):

@@ -801,3 +801,5 @@ extern "C" tasep_status tasep_step_ref_device_noalloc(int n, const double *rates
 }
 
 #include "tasep_batch_impl.cuh"
+
+#include "tasep_mlp_impl.cuh"

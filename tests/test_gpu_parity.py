@@ -11,6 +11,7 @@ import pytest
 
 import oracle as O
 import tasep_b200 as T
+from oracle import mpa
 
 pytestmark = pytest.mark.gpu
 
@@ -164,6 +165,23 @@ def test_mixed_precision_steady_state(n):
     # float stage vectors do not sum to zero exactly; the drift stays far below
     # the 1e-6 density bound
     assert abs(obs["mass"] - 1.0) <= 1e-8
+
+
+@pytest.mark.parametrize("alpha,beta", [(0.3, 0.7), (0.9, 0.9), (0.2, 0.25)])
+@pytest.mark.parametrize("precision", [T.PRECISION_FP64, T.PRECISION_MIXED])
+def test_homogeneous_steady_state_matches_matrix_product(alpha, beta, precision):
+    """Homogeneous hop rates 1: the converged profile against the exact
+    matrix-product stationary densities (low-density, maximal-current and
+    coexistence-line cases)."""
+    n = 14
+    exact = np.array(mpa.densities_float(n, alpha, beta))
+    with T.Meq(n, T.INTEGRATOR_RK4, precision) as m:
+        m.set_rates([alpha] + [1.0] * (n - 1) + [beta])
+        m.init(T.INIT_EMPTY)
+        res = m.run(0.01, 1000000, stop_tol=1e-10)
+        rho = m.observables()["rho"][::-1]  # site order
+    assert res["converged"] == 1
+    assert np.max(np.abs(rho - exact)) <= (1e-8 if precision == T.PRECISION_FP64 else 1e-6)
 
 
 @pytest.mark.parametrize("n", [2, 4, 9, 11, 12, 15, 17])

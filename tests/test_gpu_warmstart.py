@@ -1,0 +1,100 @@
+"""GPU tests of the learned warm start: the training and inference kernels
+against the CPU network oracle, the device pair-Markov measure, and what a
+trained network gains over the cold start."""
+import numpy as np
+import pytest
+
+import tasep_b200 as tb
+from oracle import mlp as omlp
+from tasep_b200 import warmstart as ws
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(seed, scale=1.0):
+    rng = np.random.default_rng(seed)
+    m = tb.Mlp(seed=seed)
+    p = m.params * scale
+    p[omlp.NPARAMS - 2:] = rng.uniform(-0.1, 0.1, 2)  # non-zero output bias
+    m.params = p
+    return m, p
+
+
+@pytest.mark.parametrize("count", [1, 63, 64, 1000, 5000])
+def test_loss_grad_matches_oracle(count):
+    m, p = _params(1)
+    rng = np.random.default_rng(count)
+    x = rng.standard_normal((count, 16)).astype(np.float32)
+    t = rng.standard_normal((count, 2)).astype(np.float32)
+    w = (1.0, 2.5)
+    loss, g = m.loss_grad(x, t, w)
+    lref, gref = omlp.loss_grad(p, x, t, w)
+    # FP32 accumulation on the GPU, float64 in the oracle, same BF16 weights
+    assert abs(loss - lref) <= 1e-5 * abs(lref)
+    assert np.abs(g - gref).max() <= 1e-4 * np.abs(gref).max()
+    m.close()
+
+
+def test_predict_matches_oracle():
+    m, p = _params(2)
+    x = np.random.default_rng(5).standard_normal((777, 16)).astype(np.float32)
+    y = m.predict(x)
+    yref, _ = omlp.forward(p, x)
+    assert np.abs(y - yref).max() <= 1e-5 * (1 + np.abs(yref).max())
+    m.close()
+
+
+def test_training_reduces_loss_and_is_deterministic():
+    rng = np.random.default_rng(7)
+    x = rng.uniform(-1, 1, (6000, 16)).astype(np.float32)
+    t = np.column_stack([np.sin(x[:, 0] + x[:, 1]) * 0.5, x[:, 2] * x[:, 3]]).astype(np.float32)
+    out = []
+    for _ in range(2):
+        m = tb.Mlp(seed=11)
+        losses = m.train(x, t, epochs=30, batch=512, lr=2e-3, seed=5)
+        out.append((losses, m.params))
+        m.close()
+    (l1, p1), (l2, p2) = out
+    assert l1[-1] < 0.1 * l1[0]
+    assert np.array_equal(l1, l2) and np.array_equal(p1, p2)
+
+
+@pytest.mark.parametrize("n", [10, 15])
+def test_pair_markov_matches_oracle(n):
+    rng = np.random.default_rng(n)
+    rho = rng.uniform(0.05, 0.95, n)
+    cov = rng.uniform(-0.03, 0.03, n - 1)
+    with tb.Meq(n, tb.INTEGRATOR_RK4) as m:
+        tb.init_pair_markov(m, rho, cov)
+        x = m.store()
+    ref = omlp.pair_markov(n, rho, cov)
+    assert np.abs(x - ref).max() <= 1e-15
+    assert abs(x.sum() - 1) < 1e-12
+
+
+def test_pair_markov_rejects_infeasible():
+    with tb.Meq(8, tb.INTEGRATOR_RK4) as m:
+        with pytest.raises(tb.TasepError) as e:
+            tb.init_pair_markov(m, np.array([0.5] * 7 + [1.0]), np.zeros(7))
+        assert e.value.status == 1
+        with pytest.raises(tb.TasepError):
+            tb.init_pair_markov(m, np.array([0.5] * 3 + [-0.2] + [0.5] * 4), np.zeros(7))
+
+
+def test_learned_start_gains_over_cold_start():
+    """Train on batched steady states at n=12 and n=13, then start n=14
+    systems from the prediction: the same steady state (densities within
+    1e-8), reached in fewer RK4 steps than from the empty lattice."""
+    data, info = ws.generate([(12, 768), (13, 512)], seed=3, max_steps=60000)
+    assert all(r["converged"] > 0.9 * r["systems"] for r in info)
+    X, Y = ws.dataset(data)
+    m = tb.Mlp(seed=0)
+    losses = ws.train(m, X, Y, schedule=((40, 1e-3), (20, 3e-4)))
+    assert losses[-1] < 0.05 * losses[0]
+    rows = ws.evaluate(m, 14, 3, seed=4)
+    m.close()
+    for r in rows:
+        assert r["cold_converged"] and r["warm_converged"] and r["start"] == "learned"
+        assert r["max_density_diff"] < 1e-8
+        assert r["prediction_density_err"] < 0.05
+    assert sum(r["warm_steps"] for r in rows) < sum(r["cold_steps"] for r in rows)
