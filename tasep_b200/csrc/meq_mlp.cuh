@@ -2,10 +2,10 @@
 // measure of the learned warm start.
 //
 // Network: 16 inputs (a window of 9 rates around the site, inverse distances to
-// both ends, the boundary rates, the smallest and the mean hop rate, and the
-// lattice length), three hidden layers of
-// 64 tanh units, 2 linear outputs (the site's density and its nearest-
-// neighbour covariance).  The forward and backward passes use BF16 copies of
+// both ends, the boundary rates, and the mean-field densities of the site and
+// its two neighbours; the host builds them), three hidden layers of 64 tanh
+// units, 2 linear outputs (the site's density and its nearest-neighbour
+// covariance).  The forward and backward passes use BF16 copies of
 // the weights and accumulate in FP32; Adam updates FP32 master weights and
 // refreshes the BF16 copies.  Each CTA writes its gradient to its own row and
 // a second kernel adds the rows in CTA order, so training is deterministic.

@@ -9,15 +9,28 @@ measure over all 2^n states, built on the device
 rule.  The empty lattice remains the fallback when a prediction is infeasible
 and the check of the converged result.
 
-Inputs of the network (16 per site j of a lattice of n sites, rates r[0..n]):
-the 9 rates r[j-4..j+4] (0 outside 0..n), 1/(j+1) and 1/(n-j), the boundary
-rates alpha = r[0] and beta = r[n], the smallest and the mean hop rate, and
-n/32.  A window of 9 rates alone cannot see the boundary rates that set the
-phase of sites far from the ends, hence the global terms.  Outputs: rho_j and
-10 * (<tau_j tau_(j+1)> - rho_j rho_(j+1)) (0 for the last site).
+Inputs of the network (16 per site j of a lattice of n sites, rates r[0..n],
+r[0] = alpha the entry rate, r[i] the hop rate from site i-1 to i, r[n] =
+beta the exit rate):
+  * the 9 rates r[j-4..j+4] (0 outside 0..n);
+  * the distances to both ends as 1/(j+1) and 1/(n-j);
+  * alpha and beta;
+  * the mean-field densities of sites j-1, j, j+1 (0 left of the lattice, 1
+    right of it).
+A window of rates cannot see a bottleneck outside it, yet the slowest bond
+decides whether a site sits in a jam (upstream) or a depleted stretch
+(downstream).  The mean-field profile (mean_field_profile: the current
+J_i = r_i rho_(i-1) (1 - rho_i) relaxed to a constant) carries that global
+information cheaply; the network corrects it towards the master equation's
+profile.  The mean-field profile alone, as a product measure, is also the
+non-learned start the learned one is compared with.
+
+Outputs: rho_j and COV_SCALE * (<tau_j tau_(j+1)> - rho_j rho_(j+1)) (0 for
+the last site).
 """
 from __future__ import annotations
 
+import os
 import time
 
 import numpy as np
@@ -25,21 +38,59 @@ import numpy as np
 from . import Batch, INIT_EMPTY, INTEGRATOR_RK4, Meq, Mlp, PRECISION_FP64, TasepError, init_pair_markov
 
 COV_SCALE = 10.0
+MF_STEPS = 20000
+# parameters trained by `python -m tasep_b200.warmstart` with its defaults:
+# 19,992 converged steady states at n = 12..20 (seed 3), 100 epochs
+PRETRAINED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warmstart_params.npy")
 
 
-def site_features(rates):
-    r = np.asarray(rates, dtype=np.float64)
-    n = len(r) - 1
-    pad = np.concatenate([np.zeros(4), r, np.zeros(4)])
-    hops = r[1:n] if n > 1 else np.array([1.0])
-    glob = [r[0], r[n], hops.min(), hops.mean(), n / 32.0]
-    f = np.empty((n, 16), dtype=np.float32)
+def pretrained(device=-1):
+    """The shipped trained network on `device`."""
+    m = Mlp(seed=0, device=device)
+    m.params = np.load(PRETRAINED)
+    return m
+
+
+def mean_field_profile(rates, steps=MF_STEPS):
+    """Mean-field densities for one rate vector (n+1,) or a batch (count, n+1).
+
+    Explicit Euler on d rho_i/dt = J_i - J_(i+1) with J_0 = alpha (1 - rho_0),
+    J_i = r_i rho_(i-1) (1 - rho_i), J_n = beta rho_(n-1), from rho = 1/2, with
+    dt = 1/(4 max rate) for a fixed number of steps (deterministic; the slow
+    modes of long lattices are not fully relaxed, which does not matter for a
+    feature)."""
+    R = np.atleast_2d(np.asarray(rates, dtype=np.float64))
+    c, n1 = R.shape
+    n = n1 - 1
+    dt = 0.25 / R.max(axis=1, keepdims=True)
+    rho = np.full((c, n), 0.5)
+    J = np.empty((c, n + 1))
+    for _ in range(steps):
+        J[:, 0] = R[:, 0] * (1.0 - rho[:, 0])
+        J[:, 1:n] = R[:, 1:n] * rho[:, :-1] * (1.0 - rho[:, 1:])
+        J[:, n] = R[:, n] * rho[:, -1]
+        rho += dt * (J[:, :-1] - J[:, 1:])
+    rho = np.clip(rho, 1e-6, 1.0 - 1e-6)
+    return rho[0] if np.ndim(rates) == 1 else rho
+
+
+def site_features(rates, mf=None):
+    """(n, 16) network inputs of one rate vector, or (count, n, 16) of a batch."""
+    R = np.atleast_2d(np.asarray(rates, dtype=np.float64))
+    c, n1 = R.shape
+    n = n1 - 1
+    rho = np.atleast_2d(mean_field_profile(R) if mf is None else mf)
+    pad = np.concatenate([np.zeros((c, 4)), R, np.zeros((c, 4))], axis=1)
+    rp = np.concatenate([np.zeros((c, 1)), rho, np.ones((c, 1))], axis=1)
+    f = np.empty((c, n, 16), dtype=np.float32)
     for j in range(n):
-        f[j, :9] = pad[j:j + 9]  # r[j-4] .. r[j+4]
-        f[j, 9] = 1.0 / (j + 1)
-        f[j, 10] = 1.0 / (n - j)
-        f[j, 11:] = glob
-    return f
+        f[:, j, :9] = pad[:, j:j + 9]  # r[j-4] .. r[j+4]
+        f[:, j, 9] = 1.0 / (j + 1)
+        f[:, j, 10] = 1.0 / (n - j)
+        f[:, j, 11] = R[:, 0]
+        f[:, j, 12] = R[:, n]
+        f[:, j, 13:16] = rp[:, j:j + 3]  # mean-field rho_(j-1), rho_j, rho_(j+1)
+    return f[0] if np.ndim(rates) == 1 else f
 
 
 def profile_targets(x, n):
@@ -92,12 +143,11 @@ def dataset(data, ns=None):
     """Per-site training arrays (X (m, 16), Y (m, 2)) from generate()'s output."""
     xs, ys = [], []
     for n, (R, Y) in sorted(data.items()):
-        if ns is not None and n not in ns:
+        if (ns is not None and n not in ns) or len(R) == 0:
             continue
-        for r, y in zip(R, Y):
-            xs.append(site_features(r))
-            ys.append(y)
-    return np.concatenate(xs), np.concatenate(ys).astype(np.float32)
+        xs.append(site_features(R).reshape(-1, 16))
+        ys.append(np.asarray(Y, dtype=np.float32).reshape(-1, 2))
+    return np.concatenate(xs), np.concatenate(ys)
 
 
 def save_data(path, data):
@@ -118,11 +168,17 @@ def predict_profile(mlp, rates):
     return rho, cov[: max(n - 1, 0)]
 
 
+STARTS = ("empty", "uniform", "meanfield", "learned")
+
+
 def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, stop_tol=1e-10, device=-1):
-    """Classical RK4 (FP64) from `start` ('empty', 'uniform' or 'learned') to the
-    exit rule.  Returns (final state, run result, seconds from the start's
-    set-up - network inference and measure construction included - to the
-    end of the run, the start actually used)."""
+    """Classical RK4 (FP64) from `start` to the exit rule: 'empty' (the
+    empty lattice), 'uniform' (every state 2^-n), 'meanfield' (product
+    measure of the mean-field profile) or 'learned' (pair-Markov measure of
+    the network's prediction).  Returns (final state, run result, seconds
+    from the start's set-up - profile computation, network inference and
+    measure construction included - to the end of the run, the start
+    actually used)."""
     m = Meq(n, INTEGRATOR_RK4, PRECISION_FP64, device=device)
     try:
         m.set_rates(rates)
@@ -136,10 +192,14 @@ def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, st
             except TasepError:
                 m.init(INIT_EMPTY)  # infeasible prediction: cold start
                 used = "empty (fallback)"
+        elif start == "meanfield":
+            init_pair_markov(m, mean_field_profile(rates), np.zeros(n - 1))
         elif start == "uniform":
             init_pair_markov(m, np.full(n, 0.5), np.zeros(n - 1))
-        else:
+        elif start == "empty":
             m.init(INIT_EMPTY)
+        else:
+            raise ValueError(f"unknown start {start!r}")
         res = m.run(h, max_steps, stop_tol=stop_tol)
         seconds = time.perf_counter() - t0
         return m.store(), res, seconds, used
@@ -147,7 +207,7 @@ def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, st
         m.close()
 
 
-def train(mlp, X, Y, schedule=((60, 1e-3), (40, 3e-4), (30, 1e-4)), batch=1024, seed=0, out_weights=(1.0, 1.0)):
+def train(mlp, X, Y, schedule=((50, 3e-3), (30, 1e-3), (20, 3e-4)), batch=512, seed=0, out_weights=(1.0, 1.0)):
     """Mini-batch Adam in phases of (epochs, learning rate); returns the per-epoch losses."""
     losses = []
     for k, (epochs, lr) in enumerate(schedule):
@@ -155,30 +215,54 @@ def train(mlp, X, Y, schedule=((60, 1e-3), (40, 3e-4), (30, 1e-4)), batch=1024, 
     return losses
 
 
-def evaluate(mlp, n, count, seed=4, h=0.01, max_steps=2000000, log=None):
-    """Held-out rate vectors (a seed the training data did not use): cold and
-    learned starts to the exit rule, wall time and final profile difference."""
+def evaluate(mlp, n, count, seed=4, h=0.01, max_steps=2000000, starts=("empty", "meanfield", "learned"), log=None):
+    """Held-out rate vectors (a seed the training data did not use): every
+    start in `starts` run to the exit rule; wall time, steps and the final
+    profile's difference from the empty-lattice run, which judges the others."""
+    assert starts[0] == "empty"
     R = sample_rates(n, count, np.random.default_rng(seed))
     rows = []
     for i, r in enumerate(R):
-        xc, rc, tc, _ = run_to_steady_state(n, r, "empty", h=h, max_steps=max_steps)
-        _, rho_c, cov_c = profile_targets(xc, n)
-        del xc
+        row = {"n": n, "system": i}
+        ref = None
+        for s in starts:
+            x, res, sec, used = run_to_steady_state(n, r, s, mlp, h=h, max_steps=max_steps)
+            _, rho, cov = profile_targets(x, n)
+            del x
+            if ref is None:
+                ref = (rho, cov)
+            row[s] = {"start": used, "seconds": round(sec, 4), "steps": int(res["steps_done"]),
+                      "converged": bool(res["converged"]),
+                      "max_density_diff": float(np.abs(rho - ref[0]).max()),
+                      "max_cov_diff": float(np.abs(cov - ref[1]).max())}
         rho_p, cov_p = predict_profile(mlp, r)
-        xw, rw, tw, used = run_to_steady_state(n, r, "learned", mlp, h=h, max_steps=max_steps)
-        _, rho_w, cov_w = profile_targets(xw, n)
-        del xw
-        rows.append({"n": n, "system": i, "start": used, "cold_seconds": round(tc, 4), "warm_seconds": round(tw, 4),
-                     "cold_steps": int(rc["steps_done"]), "warm_steps": int(rw["steps_done"]),
-                     "cold_converged": bool(rc["converged"]), "warm_converged": bool(rw["converged"]),
-                     "speedup": round(tc / tw, 3),
-                     "max_density_diff": float(np.abs(rho_c - rho_w).max()),
-                     "max_cov_diff": float(np.abs(cov_c - cov_w).max()),
-                     "prediction_density_err": float(np.abs(rho_p - rho_c).max()),
-                     "prediction_cov_err": float(np.abs(cov_p - cov_c[: n - 1]).max())})
+        row["prediction_density_err"] = float(np.abs(rho_p - ref[0]).max())
+        row["prediction_cov_err"] = float(np.abs(cov_p - ref[1][: n - 1]).max())
+        row["meanfield_density_err"] = float(np.abs(mean_field_profile(r) - ref[0]).max())
+        for s in starts[1:]:
+            row[s]["speedup"] = round(row["empty"]["seconds"] / row[s]["seconds"], 3)
+        rows.append(row)
         if log:
-            log(rows[-1])
+            log(row)
     return rows
+
+
+def summarize(rows, starts=("empty", "meanfield", "learned")):
+    out = {}
+    for n in sorted({r["n"] for r in rows}):
+        rs = [r for r in rows if r["n"] == n]
+        tc = sum(r["empty"]["seconds"] for r in rs)
+        s = {"systems": len(rs), "empty_seconds": round(tc, 3),
+             "prediction_density_err_median": float(np.median([r["prediction_density_err"] for r in rs])),
+             "meanfield_density_err_median": float(np.median([r["meanfield_density_err"] for r in rs]))}
+        for st in starts[1:]:
+            tw = sum(r[st]["seconds"] for r in rs)
+            s[st] = {"seconds": round(tw, 3), "wall_time_ratio": round(tc / tw, 3),
+                     "step_ratio": round(sum(r["empty"]["steps"] for r in rs) / sum(r[st]["steps"] for r in rs), 3),
+                     "max_density_diff": max(r[st]["max_density_diff"] for r in rs),
+                     "all_converged": all(r[st]["converged"] for r in rs)}
+        out[f"n{n}"] = s
+    return out
 
 
 def _pairs(text):
@@ -191,8 +275,8 @@ def main(argv=None):
     import os
 
     ap = argparse.ArgumentParser(description="train the warm-start network on batched steady states and "
-                                             "compare learned and cold starts")
-    ap.add_argument("--sizes", default="12:8000,14:6000,16:4000,18:1500,20:500", help="n:systems,...")
+                                             "compare learned, mean-field and cold starts")
+    ap.add_argument("--sizes", default="12:6000,13:4000,14:3500,16:3000,18:2500,20:1000", help="n:systems,...")
     ap.add_argument("--data", default=None, help="dataset .npz (read if present, else generated and written)")
     ap.add_argument("--params", default=None, help="trained parameters .npy (read if present, else trained)")
     ap.add_argument("--eval", default="24:8", help="held-out n:count,...")
@@ -216,13 +300,15 @@ def main(argv=None):
     # hold out every tenth system of each size for the validation loss
     train_d = {n: (R[np.arange(len(R)) % 10 != 0], Y[np.arange(len(R)) % 10 != 0]) for n, (R, Y) in data.items()}
     val_d = {n: (R[::10], Y[::10]) for n, (R, Y) in data.items()}
+    t0 = time.time()
     X, Y = dataset(train_d)
     Xv, Yv = dataset(val_d)
+    report["feature_seconds"] = round(time.time() - t0, 2)
     mlp = Mlp(seed=0)
     if a.params and os.path.exists(a.params):
         mlp.params = np.load(a.params)
     else:
-        sched = [(max(1, int(round(e * a.epochs))), lr) for e, lr in ((60, 1e-3), (40, 3e-4), (30, 1e-4))]
+        sched = [(max(1, int(round(e * a.epochs))), lr) for e, lr in ((50, 3e-3), (30, 1e-3), (20, 3e-4))]
         t0 = time.time()
         losses = train(mlp, X, Y, schedule=sched)
         report["train_seconds"] = round(time.time() - t0, 2)
@@ -232,22 +318,16 @@ def main(argv=None):
     report["train_samples"] = int(len(X))
     report["val_loss"] = mlp.loss_grad(Xv, Yv)[0]
     P = mlp.predict(Xv)
-    report["val_max_density_err"] = float(np.abs(P[:, 0] - Yv[:, 0]).max())
     report["val_mean_density_err"] = float(np.abs(P[:, 0] - Yv[:, 0]).mean())
+    report["val_max_density_err"] = float(np.abs(P[:, 0] - Yv[:, 0]).max())
+    report["val_meanfield_mean_density_err"] = float(np.abs(Xv[:, 14] - Yv[:, 0]).mean())
     log({k: report[k] for k in report if k != "generate"})
     rows = []
     for n, count in _pairs(a.eval):
         rows += evaluate(mlp, n, count, log=log)
     report["eval"] = rows
-    for n in sorted({r["n"] for r in rows}):
-        rs = [r for r in rows if r["n"] == n]
-        tc, tw = sum(r["cold_seconds"] for r in rs), sum(r["warm_seconds"] for r in rs)
-        report[f"summary_n{n}"] = {"systems": len(rs), "cold_seconds": round(tc, 3), "warm_seconds": round(tw, 3),
-                                   "wall_time_ratio": round(tc / tw, 3),
-                                   "median_speedup": float(np.median([r["speedup"] for r in rs])),
-                                   "max_density_diff": max(r["max_density_diff"] for r in rs),
-                                   "all_converged": all(r["cold_converged"] and r["warm_converged"] for r in rs)}
-        log(report[f"summary_n{n}"])
+    report["summary"] = summarize(rows)
+    log(report["summary"])
     if a.out:
         with open(a.out, "w") as f:
             json.dump(report, f, indent=1)

@@ -81,20 +81,25 @@ def test_pair_markov_rejects_infeasible():
             tb.init_pair_markov(m, np.array([0.5] * 3 + [-0.2] + [0.5] * 4), np.zeros(7))
 
 
-def test_learned_start_gains_over_cold_start():
-    """Train on batched steady states at n=12 and n=13, then start n=14
-    systems from the prediction: the same steady state (densities within
-    1e-8), reached in fewer RK4 steps than from the empty lattice."""
-    data, info = ws.generate([(12, 768), (13, 512)], seed=3, max_steps=60000)
+def test_learned_start_gains_over_cold_and_meanfield_starts():
+    """Train on batched steady states at n=12 and n=13, then start held-out
+    n=14 systems from the prediction.  Every start reaches the empty-lattice
+    run's steady state; the learned start needs fewer RK4 steps than the empty
+    lattice, and its predicted profile is closer to the steady state than the
+    mean-field profile the network is given as input."""
+    data, info = ws.generate([(12, 1500), (13, 1000)], seed=3, max_steps=60000)
     assert all(r["converged"] > 0.9 * r["systems"] for r in info)
     X, Y = ws.dataset(data)
     m = tb.Mlp(seed=0)
-    losses = ws.train(m, X, Y, schedule=((40, 1e-3), (20, 3e-4)))
-    assert losses[-1] < 0.05 * losses[0]
-    rows = ws.evaluate(m, 14, 3, seed=4)
+    losses = ws.train(m, X, Y, schedule=((30, 3e-3), (15, 1e-3)))
+    assert losses[-1] < 0.3 * losses[0]
+    rows = ws.evaluate(m, 14, 4, seed=4)
     m.close()
+    print(ws.summarize(rows))
     for r in rows:
-        assert r["cold_converged"] and r["warm_converged"] and r["start"] == "learned"
-        assert r["max_density_diff"] < 1e-8
-        assert r["prediction_density_err"] < 0.05
-    assert sum(r["warm_steps"] for r in rows) < sum(r["cold_steps"] for r in rows)
+        assert r["empty"]["converged"] and r["learned"]["start"] == "learned"
+        for s in ("meanfield", "learned"):
+            assert r[s]["converged"] and r[s]["max_density_diff"] < 1e-8
+    assert sum(r["learned"]["steps"] for r in rows) < sum(r["empty"]["steps"] for r in rows)
+    assert np.median([r["prediction_density_err"] for r in rows]) < np.median(
+        [r["meanfield_density_err"] for r in rows])

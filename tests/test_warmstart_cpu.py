@@ -56,16 +56,33 @@ def test_pair_markov_marginals():
 def test_features_and_targets():
     rates = np.arange(1, 12, dtype=np.float64) / 10  # n = 10
     f = ws.site_features(rates)
+    mf = ws.mean_field_profile(rates)
     assert f.shape == (10, 16)
     assert np.allclose(f[0, :9], [0, 0, 0, 0, 0.1, 0.2, 0.3, 0.4, 0.5])
     assert np.allclose(f[9, :9], [0.6, 0.7, 0.8, 0.9, 1.0, 1.1, 0, 0, 0])
     assert np.allclose(f[3, 9:11], [1 / 4, 1 / 7])
-    assert np.allclose(f[5, 11:], [0.1, 1.1, 0.2, 0.6, 10 / 32])
+    assert np.allclose(f[5, 11:13], [0.1, 1.1])
+    assert np.allclose(f[5, 13:16], mf[4:7])
+    assert np.allclose(f[0, 13], 0) and np.allclose(f[9, 15], 1)
+    # a batch gives the rows of the single calls
+    R = np.stack([rates, rates[::-1]])
+    assert np.array_equal(ws.site_features(R)[1], ws.site_features(rates[::-1]))
     # an empty lattice has zero densities and covariances
     x = np.zeros(1 << 10)
     x[0] = 1
     y, rho, cov = ws.profile_targets(x, 10)
     assert not y.any()
+
+
+def test_mean_field_profile():
+    # homogeneous hops 1 on the line alpha + beta = 1: the mean-field fixed
+    # point is the exact flat profile rho = alpha (J = alpha (1 - alpha))
+    r = np.array([0.3] + [1.0] * 11 + [0.7])
+    assert np.abs(ws.mean_field_profile(r) - 0.3).max() < 1e-9
+    # a slow bond in the middle: a jam upstream, depletion downstream
+    r = np.array([1.0] + [1.0] * 7 + [0.1] + [1.0] * 7 + [1.0])
+    mf = ws.mean_field_profile(r)
+    assert mf[:7].mean() > 0.8 and mf[9:].mean() < 0.2
 
 
 def test_dataset_roundtrip(tmp_path):
