@@ -269,7 +269,7 @@ def run_ours(args):
             with open(tp) as f:
                 tr = json.load(f)
             k = f"{name}/{args.precision}"
-            if k in tr:
+            if k in tr and tr[k].get("n") == n:  # measured on this workload size only
                 traffic = tr[k]["bytes_per_state"] * N
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
