@@ -121,6 +121,17 @@ tasep_status tasep_meq_load(tasep_meq *m, const double *host_x);
  * (src/lib/solv.c:3-135).  Blocks until the loop ends. */
 tasep_status tasep_meq_run(tasep_meq *m, const tasep_run_config *rc, tasep_run_result *res);
 
+/* The same loop with snapshots, for the animation branch of the reference
+ * (-a R, src/masterEquation.c:646-666, :900-918, :949-966): after every step
+ * whose 0-based index is a multiple of `every`, and before that step's exit
+ * test takes effect, the loop calls fn(m, step, t, user) with the state of
+ * that step current on the device (t = time after the step).  The hook may
+ * call tasep_meq_observables and tasep_meq_store on the handle; it must not
+ * run or change the state. */
+typedef void (*tasep_snapshot_fn)(tasep_meq *m, uint64_t step, double t, void *user);
+tasep_status tasep_meq_run_snapshots(tasep_meq *m, const tasep_run_config *rc, uint64_t every,
+                                     tasep_snapshot_fn fn, void *user, tasep_run_result *res);
+
 /* Enqueues `steps` steps on the handle's stream without the exit rule and
  * without waiting (benchmarks, CUDA-graph capture); t advances by h. */
 tasep_status tasep_meq_enqueue_steps(tasep_meq *m, double t0, double h, uint64_t steps);

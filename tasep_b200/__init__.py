@@ -36,7 +36,7 @@ EXPORTS = (
     "tasep_step_ref_device_noalloc", "tasep_batch_create", "tasep_batch_destroy", "tasep_batch_set_rates",
     "tasep_batch_init", "tasep_batch_load", "tasep_batch_run", "tasep_batch_store", "tasep_batch_densities",
     "tasep_mlp_create", "tasep_mlp_destroy", "tasep_mlp_set_params", "tasep_mlp_get_params", "tasep_mlp_loss_grad",
-    "tasep_mlp_train", "tasep_mlp_predict", "tasep_meq_init_pair_markov",
+    "tasep_mlp_train", "tasep_mlp_predict", "tasep_meq_init_pair_markov", "tasep_meq_run_snapshots",
 )
 
 
@@ -170,6 +170,28 @@ class Meq:
         rc = _RunCfg(t0, h, steps, stop_tol, stop_count, int(bool(exit_rule)))
         res = RunResult()
         _check(lib().tasep_meq_run(self._h, C.byref(rc), C.byref(res)))
+        return res.as_dict()
+
+    def run_snapshots(self, h, steps, every, fn, t0=0.0, stop_tol=1e-10, stop_count=100, exit_rule=True):
+        """run() calling fn(self, step, t) after every step whose index is a multiple of `every`."""
+        L = lib()
+        hook_t = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, C.c_void_p)
+        L.tasep_meq_run_snapshots.argtypes = [C.c_void_p, C.POINTER(_RunCfg), C.c_uint64, hook_t, C.c_void_p,
+                                              C.POINTER(RunResult)]
+        errors = []
+
+        def hook(_h, step, t, _u):
+            try:
+                fn(self, step, t)
+            except Exception as e:  # an exception cannot cross the C frame
+                errors.append(e)
+
+        cb = hook_t(hook)
+        rc = _RunCfg(t0, h, steps, stop_tol, stop_count, int(bool(exit_rule)))
+        res = RunResult()
+        _check(L.tasep_meq_run_snapshots(self._h, C.byref(rc), every, cb, None, C.byref(res)))
+        if errors:
+            raise errors[0]
         return res.as_dict()
 
     def enqueue_steps(self, h, steps, t0=0.0):

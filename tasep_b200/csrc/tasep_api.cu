@@ -519,6 +519,63 @@ tasep_status tasep_meq_run(tasep_meq *m, const tasep_run_config *rc, tasep_run_r
     return TASEP_OK;
 }
 
+tasep_status tasep_meq_run_snapshots(tasep_meq *m, const tasep_run_config *rc, uint64_t every,
+                                     tasep_snapshot_fn fn, void *user, tasep_run_result *res) {
+    if (!valid_handle(m) || !rc || !res || !fn || every < 1) return fail(TASEP_ERR_INVALID, "bad argument");
+    tasep_status s = check_ready(m, rc->h);
+    if (s) return s;
+    CU_TRY(cudaSetDevice(m->device));
+    memset(res, 0, sizeof *res);
+    const double thresh = rc->stop_tol * rc->h;
+    CU_TRY(cudaMemsetAsync(m->ex, 0, sizeof(ExitState), m->stream));
+    const int cur0 = m->cur;
+    const bool small = m->n <= kSmallMaxN;
+    const int shift = 30 - m->n;
+    const unsigned long long chunk = shift >= 10 ? 1024ull : (shift <= 2 ? 4ull : (1ull << shift));
+    double t = rc->t0;
+    unsigned long long i = 0;
+    while (i < rc->steps) {
+        // run steps i..last: up to the next snapshot step, the end, or a chunk
+        const unsigned long long snap = (i + every - 1) / every * every;
+        unsigned long long last = std::min<unsigned long long>(snap, rc->steps - 1);
+        if (!small) last = std::min(last, i + chunk - 1);
+        if (small) {
+            if ((s = small_run(m, t, rc->h, last - i + 1, i, thresh, rc->stop_count, rc->exit_rule))) return s;
+            for (unsigned long long j = i; j <= last; ++j) t += rc->h;
+        } else {
+            for (unsigned long long j = i; j <= last; ++j) {
+                if ((s = enqueue_step(m, j, t, rc->h, thresh, rc->stop_count, rc->exit_rule))) return s;
+                t += rc->h;
+            }
+        }
+        i = last + 1;
+        CU_TRY(cudaMemcpyAsync(m->ex_host, m->ex, sizeof(ExitState), cudaMemcpyDeviceToHost, m->stream));
+        CU_TRY(cudaStreamSynchronize(m->stream));
+        const ExitState e = *m->ex_host;
+        if (e.error) return fail(TASEP_ERR_TIMEOUT, "a bounded device wait expired during the integration");
+        if (last % every == 0 && e.steps_done > last) {  // step `last` ran: snapshot it
+            if (m->prof && (s = prof_flush(m))) return s;
+            fn(m, last, t, user);
+        }
+        if (e.done) break;
+    }
+    if (m->prof && (s = prof_flush(m))) return s;
+    CU_TRY(cudaMemcpy(m->ex_host, m->ex, sizeof(ExitState), cudaMemcpyDeviceToHost));
+    const ExitState &e = *m->ex_host;
+    if (e.error) return fail(TASEP_ERR_TIMEOUT, "a bounded device wait expired during the integration");
+    const unsigned long long done = e.steps_done;
+    if (m->integrator == TASEP_INTEGRATOR_REF && !small) m->cur = int((cur0 + done) & 1ull);
+    res->steps_done = done;
+    res->steps_at_stop = e.steps_at_stop;
+    res->early_stop = e.early_stop;
+    res->converged = e.converged;
+    res->last_checksum = e.last_checksum;
+    double tt = rc->t0;
+    for (unsigned long long k = 0; k < done; ++k) tt += rc->h;
+    res->t_end = tt;
+    return TASEP_OK;
+}
+
 tasep_status tasep_meq_enqueue_steps(tasep_meq *m, double t0, double h, uint64_t steps) {
     if (!valid_handle(m)) return fail(TASEP_ERR_INVALID, "null handle");
     tasep_status s = check_ready(m, h);

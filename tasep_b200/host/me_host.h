@@ -31,8 +31,35 @@ typedef struct {
  * `threads` threads; the file is written in index order. */
 int me_write_probs(const char *path, int n, const double *x, int threads);
 
-/* The remaining files of src/masterEquation.c:1042-1539. */
-void me_write_prb_txt(const char *path);
+/* Snapshots of the -a option, one per step whose index is a multiple of the
+ * resolution (src/masterEquation.c:646-666): the observables of each, the
+ * state itself when the probability files are selected, and the 4-site
+ * correlation values of the timed correlation file. */
+typedef struct {
+    int n;
+    uint64_t dim;
+    int keep_probs;
+    size_t count, cap;
+    me_obs *obs;   /* count entries */
+    double *probs; /* count * dim when keep_probs */
+    double *corr;  /* count * (n - 5) */
+    double *buf;   /* dim doubles of scratch */
+} me_snaps;
+
+/* high_order_corr (src/masterEquation.c:47-75) evaluated on a full state
+ * vector: the correlation coefficient of the window around bits
+ * offset..offset+key_size-1. */
+double me_state_corr(const double *x, int n, int key, int key_size, int offset);
+
+/* The remaining files of src/masterEquation.c:1042-1539.  dt is the time the
+ * reference assigns between snapshots (h times the resolution). */
+void me_write_prb_txt(const char *path, const me_snaps *s, double dt);
+void me_write_exp_timed(const char *o_filename, const me_snaps *s, double dt);
+/* <o>_covariance_data/ (mul = 0) or <o>_multExpval_data/ (mul = 1):
+ * <o>_fin.ppm, one <o>_<time>.ppm per snapshot and <o>_all.txt
+ * (src/masterEquation.c:1197-1279, 1345-1417). */
+void me_write_anim_dir(const char *o_filename, int mul, const me_obs *fin, const me_snaps *s, double dt);
+void me_write_highcorr_timed(const char *o_filename, const me_snaps *s, double dt);
 void me_write_exp_values(const char *o_filename, const me_obs *ob);
 void me_write_cov(const char *path_mat, const char *path_ppm, const me_obs *ob);
 void me_write_mul(const char *path_mat, const char *path_ppm, const me_obs *ob);

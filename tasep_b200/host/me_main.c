@@ -115,6 +115,35 @@ static int read_prob_file(const char *path, int n, double *x) {
     return seen == dim ? 0 : -2;
 }
 
+/* Snapshot of -a (src/masterEquation.c:646-666): densities, covariance and
+ * product matrices from the device, the state itself for the 4-site
+ * correlations of the timed correlation file and, when probabilities are
+ * saved, for the probability snapshot file. */
+static void snapshot_hook(tasep_meq *m, uint64_t step, double t, void *user) {
+    (void)step;
+    (void)t;
+    me_snaps *s = (me_snaps *)user;
+    const int n = s->n, vals = n > 5 ? n - 5 : 0;
+    if (s->count == s->cap) {
+        s->cap = s->cap ? 2 * s->cap : 16;
+        s->obs = (me_obs *)realloc(s->obs, sizeof(me_obs) * s->cap);
+        s->corr = (double *)realloc(s->corr, sizeof(double) * (vals ? vals : 1) * s->cap);
+        if (s->keep_probs) s->probs = (double *)realloc(s->probs, sizeof(double) * s->dim * s->cap);
+        if (!s->obs || !s->corr || (s->keep_probs && !s->probs))
+            me_err_exit("ERROR: Not Enough memory to allocate animation data array", -1);
+    }
+    me_obs *ob = &s->obs[s->count];
+    memset(ob, 0, sizeof *ob);
+    ob->n = n;
+    double mass = 0;
+    if (tasep_meq_observables(m, ob->y, ob->cov, ob->mul, n >= 4 ? ob->p4 : NULL, &mass) != TASEP_OK)
+        tasep_fail("snapshot observables");
+    if (tasep_meq_store(m, s->buf, 0, s->dim) != TASEP_OK) tasep_fail("snapshot copy");
+    for (int k = 1; k <= vals; k++) s->corr[s->count * vals + (k - 1)] = me_state_corr(s->buf, n, 15, 4, n - 4 - k);
+    if (s->keep_probs) memcpy(s->probs + s->count * s->dim, s->buf, sizeof(double) * s->dim);
+    s->count++;
+}
+
 static double wall(void) {
     struct timeval tv;
     gettimeofday(&tv, NULL);
@@ -296,8 +325,8 @@ int main(int argc, char *argv[]) {
     }
     printf("Allocated calculation vectors\n");
     if (a_found) {
-        fprintf(stderr, "CAUTION: -a %d: snapshots are not written by this program; only the final state is.\n",
-                animation_resolution);
+        if (animation_resolution < 1) me_err_exit("ERROR: -a needs a positive number of steps", -1);
+        printf("Allocatng memory for animation data\n");
     }
     printf("Number of threads to be used: %d\n", num_threads);
 
@@ -402,6 +431,8 @@ int main(int argc, char *argv[]) {
     /* run in chunks so that a progress line can be printed */
     tasep_run_result rr;
     memset(&rr, 0, sizeof rr);
+    me_snaps snaps;
+    memset(&snaps, 0, sizeof snaps);
     double tt = t;
     uint64_t done = 0;
     int early_stop = 0;
@@ -409,7 +440,18 @@ int main(int argc, char *argv[]) {
     double checksum = 0;
     {
         tasep_run_config rc = {tt, h, steps, stop_condition, stop_count, time_var_found ? 0 : 1};
-        if (tasep_meq_run(m, &rc, &rr) != TASEP_OK) tasep_fail("integration");
+        if (a_found) {
+            snaps.n = n;
+            snaps.dim = dim;
+            snaps.keep_probs = save_p;
+            snaps.buf = (double *)malloc(sizeof(double) * dim);
+            if (snaps.buf == NULL) me_err_exit("ERROR: Not Enough memory to allocate animation data array", -1);
+            if (tasep_meq_run_snapshots(m, &rc, (uint64_t)animation_resolution, snapshot_hook, &snaps, &rr) !=
+                TASEP_OK)
+                tasep_fail("integration");
+        } else if (tasep_meq_run(m, &rc, &rr) != TASEP_OK) {
+            tasep_fail("integration");
+        }
         done = rr.steps_done;
         early_stop = rr.early_stop;
         steps_at_stop = rr.steps_at_stop;
@@ -454,15 +496,19 @@ int main(int argc, char *argv[]) {
     if (save_p) {
         if (me_write_probs(o_filename, n, x, num_threads) != 0) printf("ERROR: Cant write to %s\n", o_filename);
         snprintf(name, olen + 32, "%s_prb.txt", o_filename);
-        me_write_prb_txt(name);
+        me_write_prb_txt(name, a_found ? &snaps : NULL, h * animation_resolution);
     }
-    if (save_e) me_write_exp_values(o_filename, &ob);
+    if (save_e) {
+        me_write_exp_values(o_filename, &ob);
+        if (a_found) me_write_exp_timed(o_filename, &snaps, h * animation_resolution);
+    }
     if (save_c) {
         char *ppm = (char *)malloc(olen + 32);
         snprintf(name, olen + 32, "%s_cov.mat", o_filename);
         snprintf(ppm, olen + 32, "%s_cov.ppm", o_filename);
         me_write_cov(name, ppm, &ob);
         free(ppm);
+        if (a_found) me_write_anim_dir(o_filename, 0, &ob, &snaps, h * animation_resolution);
     }
     if (save_m) {
         /* With the default selection the reference sizes this name for "_cov.ppm"
@@ -480,9 +526,17 @@ int main(int argc, char *argv[]) {
         }
         me_write_mul(name, ppm, &ob);
         free(ppm);
+        if (a_found) me_write_anim_dir(o_filename, 1, &ob, &snaps, h * animation_resolution);
     }
     free(name);
     if (n >= 4) me_write_windows(o_filename, &ob);
+    if (a_found) {
+        me_write_highcorr_timed(o_filename, &snaps, h * animation_resolution);
+        free(snaps.obs);
+        free(snaps.probs);
+        free(snaps.corr);
+        free(snaps.buf);
+    }
 
     free(x);
     free(rates);

@@ -13,6 +13,7 @@
 #include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
 #include <time.h>
 
 void me_err_exit(const char *msg, int code) {
@@ -103,11 +104,56 @@ int me_write_probs(const char *path, int n, const double *x, int threads) {
     return 0;
 }
 
-void me_write_prb_txt(const char *path) {
+void me_write_prb_txt(const char *path, const me_snaps *s, double dt) {
     /* per-snapshot probabilities; empty without -a (src/masterEquation.c:1047-1062) */
     FILE *f = fopen(path, "w");
-    if (f) fclose(f);
-    else printf("ERROR: Cant write to %s\n", path);
+    if (!f) {
+        printf("ERROR: Cant write to %s\n", path);
+        return;
+    }
+    if (s && s->keep_probs) {
+        for (size_t i = 0; i < s->count; i++) {
+            const double *p = s->probs + i * s->dim;
+            fprintf(f, "%f, ", dt * (double)i);
+            for (uint64_t k = 0; k + 1 < s->dim; k++) fprintf(f, "%f, ", p[k]);
+            fprintf(f, "%f\n", p[s->dim - 1]);
+        }
+    }
+    fclose(f);
+}
+
+void me_write_exp_timed(const char *o, const me_snaps *s, double dt) {
+    const size_t size = strlen(o) + 20;
+    char *name = (char *)malloc(size);
+    snprintf(name, size, "%s_exp_timed.txt", o);
+    FILE *f = fopen(name, "w");
+    if (f) {
+        const int n = s->n;
+        for (size_t i = 0; i < s->count; i++) {
+            fprintf(f, "%f, ", dt * (double)i);
+            for (int k = 0; k < n - 1; k++) fprintf(f, "%lf, ", s->obs[i].y[n - 1 - k]);
+            fprintf(f, "%lf\n", s->obs[i].y[0]);
+        }
+        fclose(f);
+    }
+    free(name);
+}
+
+double me_state_corr(const double *x, int n, int key, int key_size, int offset) {
+    const uint64_t dim = (uint64_t)1 << n;
+    const uint64_t k_lr = ((uint64_t)key << 1) + 1 + ((uint64_t)1 << (key_size + 1));
+    const uint64_t k_le = (uint64_t)key + ((uint64_t)1 << key_size), k_re = ((uint64_t)key << 1) + 1;
+    const uint64_t m2 = ((uint64_t)1 << (key_size + 2)) - 1, m1 = ((uint64_t)1 << (key_size + 1)) - 1,
+                   m0 = ((uint64_t)1 << key_size) - 1;
+    double lr = 0, no = 0, le = 0, re = 0;
+    for (uint64_t i = 0; i < dim; i++) {
+        const uint64_t lo = i >> (offset - 1), at = i >> offset;
+        if ((lo & m2) == (k_lr & m2)) lr += x[i];
+        if ((at & m0) == ((uint64_t)key & m0)) no += x[i];
+        if ((at & m1) == (k_le & m1)) le += x[i];
+        if ((lo & m1) == (k_re & m1)) re += x[i];
+    }
+    return (lr * no - le * re) / sqrt(le * (no - le) * re * (no - re));
 }
 
 /* ---- densities ------------------------------------------------------------------ */
@@ -295,6 +341,64 @@ void me_write_windows(const char *o, const me_obs *ob) {
         for (int i = 0; i < n - mask_size + 1; i++)
             fprintf(f, "t_%d...t_%d = %lf\n", i, mask_size + i - 1,
                     me_win_point(ob, (1 << mask_size) - 1, mask_size, n - mask_size - i));
+        fclose(f);
+    }
+    free(name);
+}
+
+/* ---- snapshot directories and the timed correlation file ---------------------------- */
+
+void me_write_anim_dir(const char *o, int mul, const me_obs *fin, const me_snaps *s, double dt) {
+    const int n = s->n;
+    const size_t size = 2 * strlen(o) + 64;
+    char *dir = (char *)malloc(size), *name = (char *)malloc(size);
+    me_pixel (*colour)(double) = mul ? mul_colour : cov_colour;
+    printf(mul ? "Creating directory for mulitplicative expected values animation data\n"
+               : "Creating directory for covariance animation data\n");
+    snprintf(dir, size, mul ? "%s_multExpval_data" : "%s_covariance_data", o);
+    if (mkdir(dir, 0777) == -1) {
+        printf("Cauton: Directory <%s> already exists, Data may be overriten or lost! Continue? [Y/N]  ", dir);
+        char sel = 'N';
+        if (scanf("%c", &sel) == EOF) me_err_exit("ERROR: Issue while reading from stdin", EOF);
+        if (sel == 'N' || sel == 'n') exit(-1);
+    }
+    snprintf(name, size, "%s/%s_fin.ppm", dir, o);
+    write_map(name, n, mul ? fin->mul : fin->cov, colour);
+    printf(mul ? "Wrote final multiplicative expected values matrix ppm file to <%s>\n"
+               : "Wrote final covariance matrix ppm file to <%s>\n", name);
+    snprintf(name, size, "%s/%s_all.txt", dir, o);
+    FILE *f = fopen(name, "w");
+    if (f) {
+        for (size_t j = 0; j < s->count; j++) {
+            const double *m = mul ? s->obs[j].mul : s->obs[j].cov;
+            snprintf(name, size, "%s/%s_%lf.ppm", dir, o, dt * (double)j);
+            write_map(name, n, m, colour);
+            fprintf(f, "%d Matrix:\n", (int)j);
+            for (int i = 0; i < n; i++)
+                for (int k = 0; k < n; k++) fprintf(f, k < n - 1 ? "%lf, " : "%lf\n", m[i * n + k]);
+            fprintf(f, "\n\n");
+        }
+        fclose(f);
+    }
+    free(name);
+    free(dir);
+}
+
+void me_write_highcorr_timed(const char *o, const me_snaps *s, double dt) {
+    /* the reference sizes this name 4 characters short (src/masterEquation.c:1518-1521):
+       the file is "<o>_highcorr_timed" */
+    const int n = s->n, vals = n > 5 ? n - 5 : 0;
+    const size_t size = strlen(o) + 24;
+    char *name = (char *)malloc(size);
+    snprintf(name, size, "%s_highcorr_timed", o);
+    FILE *f = fopen(name, "w");
+    if (f) {
+        for (size_t i = 0; i < s->count; i++) {
+            printf("-->%f%%\r", 100. * (double)(i + 1) / (double)s->count);
+            fprintf(f, "%f ", dt * (double)i);
+            for (int k = 0; k < vals; k++) fprintf(f, "%1.7g ", s->corr[i * vals + k]);
+            fprintf(f, "\n");
+        }
         fclose(f);
     }
     free(name);

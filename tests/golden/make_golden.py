@@ -55,6 +55,8 @@ STOCK_CASES = {
     # time-variant rates (per-row path, no exit test)
     "n5_timevar": {"rates": (5, 13), "timevar": True,
                    "args": ["-n", "5", "-t", "0", "-T", "6", "-s", "600", "--time-var"]},
+    # snapshots every 50 steps (-a): timed files and per-snapshot matrix directories
+    "n7_anim": {"rates": (7, 14), "args": ["-n", "7", "-t", "0", "-T", "3", "-s", "300", "-f", "-a", "50"]},
 }
 
 
@@ -95,6 +97,8 @@ def run_stock(name, spec, outdir):
         for fn in sorted(os.listdir(tmp)):
             if fn.startswith("out") and os.path.isfile(os.path.join(tmp, fn)):
                 shutil.copy(os.path.join(tmp, fn), os.path.join(dst, fn))
+            elif fn.startswith("out") and os.path.isdir(os.path.join(tmp, fn)):
+                shutil.copytree(os.path.join(tmp, fn), os.path.join(dst, fn), dirs_exist_ok=True)
         with open(os.path.join(dst, "run.json"), "w") as f:
             json.dump(info, f, indent=1)
         print(name, "rc", p.returncode, "convergence", info["convergence_after"], sorted(os.listdir(dst)))
@@ -132,8 +136,12 @@ def run_mpa(outdir):
 def main():
     if not os.path.exists(O.REF_BIN):
         sys.exit("build the reference first: make -C oracle")
+    only = sys.argv[1:]  # optional: regenerate only these stock cases
     for name, spec in STOCK_CASES.items():
-        run_stock(name, spec, HERE)
+        if not only or name in only:
+            run_stock(name, spec, HERE)
+    if only:
+        return
     run_harness(HERE)
     run_mpa(HERE)
 

@@ -63,7 +63,7 @@ def test_bad_rate_file_is_reported(tmp_path):
 
 # ---------------------------------------------------------------- GPU ---------
 
-CASES = ["cfg1_f", "n7_rows", "n8_f", "n5_timevar"]
+CASES = ["cfg1_f", "n7_rows", "n8_f", "n5_timevar", "n7_anim"]
 
 
 def _prepare(name, tmp_path):
@@ -121,6 +121,38 @@ def test_drop_in_matches_stock_binary_files(name, tmp_path):
     rows = [line.split() for line in open(os.path.join(tmp_path, "out_highcorr"))]
     assert [int(v) for v in rows[0]] == list(range(1, n - 2))
     assert len(rows) == 5 and all(len(r) == n - 2 for r in rows[1:])
+
+
+@pytest.mark.gpu
+def test_drop_in_snapshots_match_stock_binary(tmp_path):
+    """-a 50: the timed density and probability files, and the per-snapshot
+    covariance and product matrices with their pictures, as the stock binary
+    wrote them (src/masterEquation.c:646-666, :1047-1110, :1197-1279,
+    :1345-1417, :1516-1536)."""
+    d, info = _prepare("n7_anim", tmp_path)
+    p = run(info["argv"] + ["--stop-tol", "1e-7"], tmp_path)
+    assert p.returncode == 0, p.stderr
+    assert "Allocatng memory for animation data" in p.stdout
+    for sub in ("out_covariance_data", "out_multExpval_data"):
+        names = sorted(os.listdir(os.path.join(d, sub)))
+        assert sorted(os.listdir(tmp_path / sub)) == names
+        for fn in names:
+            a, b = (tmp_path / sub / fn).read_bytes(), open(os.path.join(d, sub, fn), "rb").read()
+            if fn.endswith(".ppm"):
+                assert a.split(b"\n", 3)[:3] == b.split(b"\n", 3)[:3] and len(a) == len(b)
+                assert max(abs(x - y) for x, y in zip(a, b)) <= 1, (sub, fn)
+            else:
+                fa, fb = _floats(tmp_path / sub / fn), _floats(os.path.join(d, sub, fn))
+                assert fa.shape == fb.shape and np.max(np.abs(fa - fb)) <= 1.5e-6, (sub, fn)
+    for fn in ("out_exp_timed.txt", "out_prb.txt"):
+        fa, fb = _floats(tmp_path / fn), _floats(os.path.join(d, fn))
+        assert fa.size > 0 and fa.shape == fb.shape and np.max(np.abs(fa - fb)) <= 1.5e-6, fn
+    # timed 4-site correlations: same snapshot times and row lengths; the values
+    # are the correlation coefficient (the reference function returns nothing)
+    ours = [line.split() for line in open(tmp_path / "out_highcorr_timed")]
+    gold = [line.split() for line in open(os.path.join(d, "out_highcorr_timed"))]
+    assert [r[0] for r in ours] == [r[0] for r in gold]
+    assert all(len(r) == 1 + 7 - 5 for r in ours)
 
 
 @pytest.mark.gpu

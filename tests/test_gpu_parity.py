@@ -298,3 +298,44 @@ def test_steps_random_dense_state_full_size(n, integrator):
                 assert np.array_equal(y, xo), _mismatch_report(y, xo)
             else:
                 assert np.max(np.abs(y - xo)) <= PROB_TOL, _mismatch_report(y, xo)
+
+
+@pytest.mark.parametrize("n,integrator", [(9, T.INTEGRATOR_REF), (14, T.INTEGRATOR_REF), (14, T.INTEGRATOR_RK4)])
+def test_run_snapshots_matches_plain_run(n, integrator):
+    """tasep_meq_run_snapshots: the hook sees the state after steps 0, R, 2R, ...
+    and the run ends where the plain run ends."""
+    r = rates_for(n, 130 + n)
+    snaps = []
+    with T.Meq(n, integrator) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res = m.run_snapshots(0.01, 450, 100, lambda mm, step, t: snaps.append((step, t, mm.store())))
+        x = m.store()
+    assert [s for s, _, _ in snaps] == [0, 100, 200, 300, 400]
+    assert all(abs(t - 0.01 * (s + 1)) < 1e-12 for s, t, _ in snaps)
+    with T.Meq(n, integrator) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res2 = m.run(0.01, 450)
+        assert np.array_equal(m.store(), x) and res2 == res
+    oi = O.INT_REF if integrator == T.INTEGRATOR_REF else O.INT_RK4
+    for step, _, xs in snaps:
+        xo, _ = O.run(n, r, h=0.01, steps=step + 1, integrator=oi, init=O.INIT_EMPTY)
+        assert np.max(np.abs(xs - xo)) <= (0 if integrator == T.INTEGRATOR_REF else PROB_TOL)
+
+
+@pytest.mark.parametrize("n", [8, 13])
+def test_run_snapshots_stop_at_the_exit_rule(n):
+    r = rates_for(n, 150 + n)
+    steps = []
+    with T.Meq(n, T.INTEGRATOR_REF) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res = m.run_snapshots(0.01, 100000, 7, lambda mm, step, t: steps.append(step), stop_tol=1e-4)
+    with T.Meq(n, T.INTEGRATOR_REF) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res2 = m.run(0.01, 100000, stop_tol=1e-4)
+    assert res == res2 and res["converged"] == 1
+    last = res["steps_done"] - 1
+    assert steps == list(range(0, last + 1, 7))
