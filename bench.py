@@ -119,17 +119,33 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def dist_setup(gpus):
+def dist_setup(gpus, backend="nccl"):
+    """One process per GPU (torchrun): the process group only carries the
+    barrier and the max-over-ranks time; each rank integrates its own replica."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=None)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         return dist, rank, world, local
     return None, 0, 1, 0
+
+
+def max_over_ranks(dist, x, device="cuda"):
+    """The largest of every rank's x (every rank calls this at the same point)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_value(world, steps, ms):
+    """Whole-job steps/s: every replica did `steps` steps in at most `ms`."""
+    return world * steps / (ms / 1000.0)
 
 
 def cpu_baseline_sample(n, rates, h, target_s=15.0):
@@ -226,11 +242,8 @@ def run_ours(args):
     prof = m.profile_read()
     m.profile(False)
     clocks = clk.summary()
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1000.0)
+    ms = max_over_ranks(dist, ms)
+    value = replicas_value(world, args.steps, ms)
 
     # e2e through the public API with host buffers
     x_host = torch.zeros(N, dtype=torch.float64, pin_memory=True).numpy()
@@ -246,12 +259,8 @@ def run_ours(args):
     e1.record(stream)
     e1.synchronize()
     barrier()
-    ems = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ems], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ems = float(t.item())
-    e2e_value = world * args.steps / (ems / 1000.0)
+    ems = max_over_ranks(dist, e0.elapsed_time(e1))
+    e2e_value = replicas_value(world, args.steps, ems)
     mass = float(out_host.sum())
 
     # roofline of the dominant kernel
