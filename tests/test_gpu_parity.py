@@ -179,9 +179,13 @@ def test_homogeneous_steady_state_matches_matrix_product(alpha, beta, precision)
         m.set_rates([alpha] + [1.0] * (n - 1) + [beta])
         m.init(T.INIT_EMPTY)
         res = m.run(0.01, 1000000, stop_tol=1e-10)
-        rho = m.observables()["rho"][::-1]  # site order
+        obs = m.observables()
+    rho = obs["rho"][::-1]  # site order
     assert res["converged"] == 1
     assert np.max(np.abs(rho - exact)) <= (1e-8 if precision == T.PRECISION_FP64 else 1e-6)
+    # connected correlations against the exact two-point function
+    cov_exact = np.array(mpa.covariance(n, alpha, beta))
+    assert np.max(np.abs(obs["cov"] - cov_exact)) <= (1e-8 if precision == T.PRECISION_FP64 else 1e-6)
 
 
 @pytest.mark.parametrize("n", [2, 4, 9, 11, 12, 15, 17])

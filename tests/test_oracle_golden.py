@@ -197,3 +197,24 @@ def test_classical_rk4_is_fourth_order():
         errs.append(np.max(np.abs(x - xr)))
     rates_ = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
     assert min(rates_) > 3.7
+
+
+def test_mpa_representation_matches_reference_densities():
+    """The explicit matrix representation behind mpa.two_point gives the same
+    densities as the reference's B-table formula (src/steadystates_gmp.c:142-186)."""
+    for n, a, b in [(6, 0.3, 0.5), (8, 0.9, 0.9), (9, 1.2, 0.35), (10, 0.6, 0.4)]:
+        d1, d2 = mpa.densities(n, a, b), mpa.densities_ansatz(n, a, b)
+        assert max(abs(float((x - y) / x)) for x, y in zip(d1, d2)) < 1e-15
+
+
+def test_mpa_two_point_matches_converged_master_equation():
+    """Exact connected correlations against the oracle's converged RK4 state."""
+    for n, a, b in [(8, 0.9, 0.9), (8, 0.3, 0.5), (7, 1.2, 0.35)]:
+        x, res = O.run(n, [a] + [1.0] * (n - 1) + [b], h=0.01, steps=400000, integrator=O.INT_RK4,
+                       init=O.INIT_EMPTY, stop_tol=1e-10)
+        assert res["early_stop"] > 100
+        cov, _ = O.covariance(n, x)
+        assert np.max(np.abs(cov - np.array(mpa.covariance(n, a, b)))) < 1e-9
+    # on alpha + beta = 1 the measure is a product measure: no correlations
+    c = np.array(mpa.covariance(8, 0.3, 0.7))
+    assert np.max(np.abs(c - np.diag(np.diag(c)))) < 1e-15
