@@ -14,6 +14,7 @@ struct tasep_mlp {
     int device = 0;
     float *master = nullptr, *m1 = nullptr, *m2 = nullptr, *gsum = nullptr, *grows = nullptr, *loss = nullptr;
     __nv_bfloat16 *w = nullptr;
+    int *err = nullptr;  // set by a kernel whose tensor-core wait timed out
     int grow_cap = 0;
     long long adam_t = 0;
 };
@@ -33,8 +34,9 @@ tasep_status mlp_configure() {
     int dev = 0;
     cudaGetDevice(&dev);
     if (!done[dev & 63]) {
-        CU_TRY(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(MlpSmem))));
-        CU_TRY(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(MlpSmem))));
+        CU_TRY(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(kMlpForwardSmem)));
+        CU_TRY(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMlpGradSmem)));
         done[dev & 63] = true;
     }
     return TASEP_OK;
@@ -52,13 +54,22 @@ tasep_status mlp_rows(tasep_mlp *m, int rows) {
     return TASEP_OK;
 }
 
+// Reads and clears the kernels' error flag (after a synchronisation).
+tasep_status mlp_check(tasep_mlp *m) {
+    int e = 0;
+    CU_TRY(cudaMemcpy(&e, m->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!e) return TASEP_OK;
+    CU_TRY(cudaMemset(m->err, 0, sizeof(int)));
+    return fail(TASEP_ERR_TIMEOUT, "a tensor-core wait of the network kernels expired");
+}
+
 // gradient of the loss over n device-resident samples into m->gsum; mean
 // loss into *loss_host (if not NULL)
 tasep_status mlp_grad_device(tasep_mlp *m, const float *xd, const float *td, int n, const float *ow, float *loss_host) {
-    const int rows = (n + kMlpBatch - 1) / kMlpBatch;
+    const int rows = (n + kMlpTile - 1) / kMlpTile;
     tasep_status s = mlp_rows(m, rows);
     if (s) return s;
-    mlp_grad_kernel<<<rows, kMlpThreads, sizeof(MlpSmem)>>>(m->w, xd, td, n, ow[0], ow[1], m->grows, m->loss);
+    mlp_grad_kernel<<<rows, kMlpThreads, kMlpGradSmem>>>(m->w, xd, td, n, ow[0], ow[1], m->grows, m->loss, m->err);
     CU_TRY(cudaGetLastError());
     mlp_reduce_kernel<<<(kMlpParams + 255) / 256, 256>>>(m->grows, rows, m->gsum);
     CU_TRY(cudaGetLastError());
@@ -68,6 +79,7 @@ tasep_status mlp_grad_device(tasep_mlp *m, const float *xd, const float *td, int
         float tot = 0.f;
         for (float v : l) tot += v;
         *loss_host = tot;
+        return mlp_check(m);
     }
     return TASEP_OK;
 }
@@ -93,7 +105,8 @@ tasep_status tasep_mlp_create(int device, uint64_t seed, tasep_mlp **out) {
               cudaMalloc(&m->m1, sizeof(float) * kMlpParams) == cudaSuccess &&
               cudaMalloc(&m->m2, sizeof(float) * kMlpParams) == cudaSuccess &&
               cudaMalloc(&m->gsum, sizeof(float) * kMlpParams) == cudaSuccess &&
-              cudaMalloc(&m->w, sizeof(__nv_bfloat16) * kMlpParams) == cudaSuccess;
+              cudaMalloc(&m->w, sizeof(__nv_bfloat16) * kMlpParams) == cudaSuccess &&
+              cudaMalloc(&m->err, sizeof(int)) == cudaSuccess && cudaMemset(m->err, 0, sizeof(int)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         tasep_mlp_destroy(m);
@@ -124,6 +137,7 @@ tasep_status tasep_mlp_destroy(tasep_mlp *m) {
     cudaFree(m->grows);
     cudaFree(m->loss);
     cudaFree(m->w);
+    cudaFree(m->err);
     delete m;
     return TASEP_OK;
 }
@@ -160,6 +174,8 @@ tasep_status tasep_mlp_loss_grad(tasep_mlp *m, const float *x, const float *t, i
     CU_TRY(cudaMemcpy(xd, x, sizeof(float) * size_t(n) * kMlpIn, cudaMemcpyHostToDevice));
     CU_TRY(cudaMemcpy(td, t, sizeof(float) * size_t(n) * kMlpOut, cudaMemcpyHostToDevice));
     s = mlp_grad_device(m, xd, td, n, out_weights, loss);
+    if (!s && cudaDeviceSynchronize() != cudaSuccess) s = fail(TASEP_ERR_CUDA, "gradient failed");
+    if (!s) s = mlp_check(m);
     if (!s && grad) {
         cudaError_t e = cudaMemcpy(grad, m->gsum, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) s = fail(TASEP_ERR_CUDA, "%s", cudaGetErrorString(e));
@@ -213,6 +229,7 @@ tasep_status tasep_mlp_train(tasep_mlp *m, const float *x, const float *t, int n
     cudaFree(xd);
     cudaFree(td);
     if (!s && cudaDeviceSynchronize() != cudaSuccess) s = fail(TASEP_ERR_CUDA, "training failed");
+    if (!s) s = mlp_check(m);
     return s;
 }
 
@@ -226,15 +243,15 @@ tasep_status tasep_mlp_predict(tasep_mlp *m, const float *x, int n, float *y) {
     CU_TRY(cudaMalloc(&yd, sizeof(float) * size_t(n) * kMlpOut));
     cudaError_t e = cudaMemcpy(xd, x, sizeof(float) * size_t(n) * kMlpIn, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-        const int grid = std::min((n + kMlpBatch - 1) / kMlpBatch, 1024);
-        mlp_forward_kernel<<<grid, kMlpThreads, sizeof(MlpSmem)>>>(m->w, xd, yd, n);
+        const int grid = std::min((n + kMlpTile - 1) / kMlpTile, 1024);
+        mlp_forward_kernel<<<grid, kMlpThreads, kMlpForwardSmem>>>(m->w, xd, yd, n, m->err);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpy(y, yd, sizeof(float) * size_t(n) * kMlpOut, cudaMemcpyDeviceToHost);
     cudaFree(xd);
     cudaFree(yd);
     if (e != cudaSuccess) return fail(TASEP_ERR_CUDA, "prediction: %s", cudaGetErrorString(e));
-    return TASEP_OK;
+    return mlp_check(m);
 }
 
 tasep_status tasep_meq_init_pair_markov(tasep_meq *m, const double *rho, const double *cov) {

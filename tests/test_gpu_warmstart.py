@@ -20,7 +20,7 @@ def _params(seed, scale=1.0):
     return m, p
 
 
-@pytest.mark.parametrize("count", [1, 63, 64, 1000, 5000])
+@pytest.mark.parametrize("count", [1, 127, 128, 129, 1000, 5000])
 def test_loss_grad_matches_oracle(count):
     m, p = _params(1)
     rng = np.random.default_rng(count)
@@ -29,8 +29,10 @@ def test_loss_grad_matches_oracle(count):
     w = (1.0, 2.5)
     loss, g = m.loss_grad(x, t, w)
     lref, gref = omlp.loss_grad(p, x, t, w)
-    # FP32 accumulation on the GPU, float64 in the oracle, same BF16 weights
-    assert abs(loss - lref) <= 1e-5 * abs(lref)
+    # same BF16 weights; the GPU's forward GEMMs run on the tensor cores with
+    # activations split into two BF16 terms (16 significant bits) and FP32
+    # accumulation, the oracle in float64
+    assert abs(loss - lref) <= 1e-4 * abs(lref)
     assert np.abs(g - gref).max() <= 1e-4 * np.abs(gref).max()
     m.close()
 
@@ -40,7 +42,7 @@ def test_predict_matches_oracle():
     x = np.random.default_rng(5).standard_normal((777, 16)).astype(np.float32)
     y = m.predict(x)
     yref, _ = omlp.forward(p, x)
-    assert np.abs(y - yref).max() <= 1e-5 * (1 + np.abs(yref).max())
+    assert np.abs(y - yref).max() <= 1e-4 * (1 + np.abs(yref).max())
     m.close()
 
 
