@@ -191,8 +191,9 @@ tasep_status tasep_batch_densities(tasep_batch *b, double *rho);
 /* ---- learned warm start ------------------------------------------------------
  * No counterpart in the reference.  A per-site network (TASEP_MLP_IN inputs,
  * three hidden layers of 64 tanh units, 2 outputs: density and nearest-
- * neighbour covariance) trained on the GPU with the library's own forward,
- * backward and Adam kernels (BF16 weights, FP32 accumulation), and a device-
+ * neighbour covariance) trained on the GPU with the library's own forward
+ * (tcgen05 tensor cores), backward and Adam kernels (BF16 weights, FP32
+ * accumulation), and a device-
  * side builder of the pair-Markov initial measure from predicted profiles. */
 #define TASEP_MLP_IN 16
 #define TASEP_MLP_OUT 2
