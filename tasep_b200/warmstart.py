@@ -281,13 +281,29 @@ def main(argv=None):
     ap.add_argument("--params", default=None, help="trained parameters .npy (read if present, else trained)")
     ap.add_argument("--eval", default="24:8", help="held-out n:count,...")
     ap.add_argument("--epochs", type=float, default=1.0, help="scale of the default training schedule")
+    ap.add_argument("--starts", default="empty,meanfield,learned", help="starts to compare (empty first)")
     ap.add_argument("--out", default=None, help="JSON report")
     a = ap.parse_args(argv)
+    starts = tuple(a.starts.split(","))
 
     def log(rec):
         print(json.dumps(rec), flush=True)
 
     report = {}
+    if a.params and os.path.exists(a.params) and not a.data:  # evaluation of a trained network only
+        mlp = Mlp(seed=0)
+        mlp.params = np.load(a.params)
+        rows = []
+        for n, count in _pairs(a.eval):
+            rows += evaluate(mlp, n, count, starts=starts, log=log)
+        report["eval"] = rows
+        report["summary"] = summarize(rows, starts)
+        log(report["summary"])
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(report, f, indent=1)
+        mlp.close()
+        return
     if a.data and os.path.exists(a.data):
         data = load_data(a.data)
     else:
@@ -324,9 +340,9 @@ def main(argv=None):
     log({k: report[k] for k in report if k != "generate"})
     rows = []
     for n, count in _pairs(a.eval):
-        rows += evaluate(mlp, n, count, log=log)
+        rows += evaluate(mlp, n, count, starts=starts, log=log)
     report["eval"] = rows
-    report["summary"] = summarize(rows)
+    report["summary"] = summarize(rows, starts)
     log(report["summary"])
     if a.out:
         with open(a.out, "w") as f:
