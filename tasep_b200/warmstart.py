@@ -74,6 +74,52 @@ def mean_field_profile(rates, steps=MF_STEPS):
     return rho[0] if np.ndim(rates) == 1 else rho
 
 
+def pair_field_profile(rates, max_steps=MF_STEPS, tol=1e-11):
+    """Pair approximation of the steady state: nearest-neighbour pair
+    probabilities p_i(a, b) = P(tau_i = a, tau_(i+1) = b) evolved under the
+    TASEP moves that change them, with three-site probabilities closed as
+    P(a, b, c) = p_(i-1)(a, b) p_i(b, c) / P(tau_i = b) (the first closure of
+    the reference's mean-field hierarchy, src/mf_full.c).  Explicit Euler from
+    the uniform product measure, dt = 1/(4 max rate), until the largest change
+    rate falls below `tol` or `max_steps`.  Returns (densities (n,), nearest-
+    neighbour covariances (n-1,)) for one rate vector, or batched arrays."""
+    R = np.atleast_2d(np.asarray(rates, dtype=np.float64))
+    c, n1 = R.shape
+    n = n1 - 1
+    dt = 0.25 / R.max(axis=1)[:, None, None, None]
+    P = np.full((c, n - 1, 2, 2), 0.25)
+    rho = np.empty((c, n))
+    tiny = 1e-300
+    for it in range(max_steps):
+        rho[:, :n - 1] = P[:, :, 1, 0] + P[:, :, 1, 1]
+        rho[:, n - 1] = P[:, -1, 0, 1] + P[:, -1, 1, 1]
+        d = np.zeros_like(P)
+        f = R[:, 1:n] * P[:, :, 1, 0]  # hop inside pair i: site i -> i+1
+        d[:, :, 1, 0] -= f
+        d[:, :, 0, 1] += f
+        gain = np.empty((c, n - 1, 2))  # left site of pair i fills: entry, or hop from site i-1
+        gain[:, 0, :] = R[:, 0, None] * P[:, 0, 0, :]
+        lose = np.empty((c, n - 1, 2))  # right site of pair i empties: exit, or hop to site i+2
+        lose[:, -1, :] = R[:, n, None] * P[:, -1, :, 1]
+        if n > 2:
+            q0 = np.maximum(1.0 - rho[:, 1:n - 1], tiny)
+            gain[:, 1:, :] = R[:, 1:n - 1, None] * P[:, :-1, 1, 0][..., None] * P[:, 1:, 0, :] / q0[..., None]
+            q1 = np.maximum(rho[:, 1:n - 1], tiny)
+            lose[:, :-1, :] = R[:, 2:n, None] * P[:, :-1, :, 1] * (P[:, 1:, 1, 0] / q1)[..., None]
+        d[:, :, 0, :] -= gain
+        d[:, :, 1, :] += gain
+        d[:, :, :, 1] -= lose
+        d[:, :, :, 0] += lose
+        P += dt * d
+        if it % 500 == 499 and np.abs(d).max() < tol:
+            break
+    rho[:, :n - 1] = P[:, :, 1, 0] + P[:, :, 1, 1]
+    rho[:, n - 1] = P[:, -1, 0, 1] + P[:, -1, 1, 1]
+    rho = np.clip(rho, 1e-6, 1.0 - 1e-6)
+    cov = P[:, :, 1, 1] - rho[:, :-1] * rho[:, 1:]
+    return (rho[0], cov[0]) if np.ndim(rates) == 1 else (rho, cov)
+
+
 def site_features(rates, mf=None):
     """(n, 16) network inputs of one rate vector, or (count, n, 16) of a batch."""
     R = np.atleast_2d(np.asarray(rates, dtype=np.float64))
@@ -168,14 +214,15 @@ def predict_profile(mlp, rates):
     return rho, cov[: max(n - 1, 0)]
 
 
-STARTS = ("empty", "uniform", "meanfield", "learned")
+STARTS = ("empty", "uniform", "meanfield", "pairfield", "learned")
 
 
 def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, stop_tol=1e-10, device=-1):
     """Classical RK4 (FP64) from `start` to the exit rule: 'empty' (the
     empty lattice), 'uniform' (every state 2^-n), 'meanfield' (product
-    measure of the mean-field profile) or 'learned' (pair-Markov measure of
-    the network's prediction).  Returns (final state, run result, seconds
+    measure of the mean-field profile), 'pairfield' (pair-Markov measure of
+    the pair approximation) or 'learned' (pair-Markov measure of the
+    network's prediction).  Returns (final state, run result, seconds
     from the start's set-up - profile computation, network inference and
     measure construction included - to the end of the run, the start
     actually used)."""
@@ -194,6 +241,8 @@ def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, st
                 used = "empty (fallback)"
         elif start == "meanfield":
             init_pair_markov(m, mean_field_profile(rates), np.zeros(n - 1))
+        elif start == "pairfield":
+            init_pair_markov(m, *pair_field_profile(rates))
         elif start == "uniform":
             init_pair_markov(m, np.full(n, 0.5), np.zeros(n - 1))
         elif start == "empty":
@@ -239,6 +288,7 @@ def evaluate(mlp, n, count, seed=4, h=0.01, max_steps=2000000, starts=("empty", 
         row["prediction_density_err"] = float(np.abs(rho_p - ref[0]).max())
         row["prediction_cov_err"] = float(np.abs(cov_p - ref[1][: n - 1]).max())
         row["meanfield_density_err"] = float(np.abs(mean_field_profile(r) - ref[0]).max())
+        row["pairfield_density_err"] = float(np.abs(pair_field_profile(r)[0] - ref[0]).max())
         for s in starts[1:]:
             row[s]["speedup"] = round(row["empty"]["seconds"] / row[s]["seconds"], 3)
         rows.append(row)
@@ -254,7 +304,8 @@ def summarize(rows, starts=("empty", "meanfield", "learned")):
         tc = sum(r["empty"]["seconds"] for r in rs)
         s = {"systems": len(rs), "empty_seconds": round(tc, 3),
              "prediction_density_err_median": float(np.median([r["prediction_density_err"] for r in rs])),
-             "meanfield_density_err_median": float(np.median([r["meanfield_density_err"] for r in rs]))}
+             "meanfield_density_err_median": float(np.median([r["meanfield_density_err"] for r in rs])),
+             "pairfield_density_err_median": float(np.median([r["pairfield_density_err"] for r in rs]))}
         for st in starts[1:]:
             tw = sum(r[st]["seconds"] for r in rs)
             s[st] = {"seconds": round(tw, 3), "wall_time_ratio": round(tc / tw, 3),

@@ -97,3 +97,25 @@ def test_dataset_roundtrip(tmp_path):
     assert R.shape == (100, 21)
     assert R[:, [0, 20]].min() >= 0.05 and R[:, [0, 20]].max() <= 1.5
     assert R[:, 1:20].min() >= 0.1 and R[:, 1:20].max() <= 5.0
+
+
+def test_pair_field_profile():
+    from oracle import mpa
+    # exact on alpha + beta = 1 (product measure): density alpha, no correlations
+    r = np.array([0.3] + [1.0] * 9 + [0.7])
+    rho, cov = ws.pair_field_profile(r)
+    assert np.abs(rho - 0.3).max() < 1e-9 and np.abs(cov).max() < 1e-9
+    # maximal current: closer to the exact densities than first-order mean field,
+    # and nearest-neighbour covariances of the right size
+    n = 10
+    r = np.array([0.9] + [1.0] * (n - 1) + [0.9])
+    exact = np.array(mpa.densities_float(n, 0.9, 0.9))
+    C = np.array(mpa.covariance(n, 0.9, 0.9))
+    rho, cov = ws.pair_field_profile(r)
+    assert np.abs(rho - exact).max() < np.abs(ws.mean_field_profile(r) - exact).max()
+    assert np.abs(cov - np.diag(C, 1)).max() < 0.02
+    # batched rows equal single calls
+    R = ws.sample_rates(12, 3, np.random.default_rng(1))
+    rb, cb = ws.pair_field_profile(R, max_steps=3000)
+    r1, c1 = ws.pair_field_profile(R[2], max_steps=3000)
+    assert np.allclose(rb[2], r1) and np.allclose(cb[2], c1)
