@@ -30,6 +30,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -40,7 +41,7 @@ sys.path.insert(0, ROOT)
 METRIC = "RK4 steps/s at n=28 (FP64 classical RK4, 4 generator applications per step)"
 UNIT = "steps/s"
 
-# algorithmic bytes per state for each kernel ("Kernels")
+# algorithmic bytes per state of each kernel: the vectors it must read and write once
 ALG_BYTES = {
     ("meq_ref_step", 0): 16, ("meq_rk4_h1", 0): 16, ("meq_rk4_h2", 0): 16, ("meq_rk4_h3", 0): 24,
     ("meq_rk4_h4", 0): 32, ("meq_rk4_h1", 1): 12, ("meq_rk4_h2", 1): 8, ("meq_rk4_h3", 1): 12,
@@ -72,7 +73,7 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f".clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"tasep_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:

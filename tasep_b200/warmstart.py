@@ -267,7 +267,7 @@ def train(mlp, X, Y, schedule=((50, 3e-3), (30, 1e-3), (20, 3e-4)), batch=512, s
 def evaluate(mlp, n, count, seed=4, h=0.01, max_steps=2000000, starts=("empty", "meanfield", "learned"), log=None):
     """Held-out rate vectors (a seed the training data did not use): every
     start in `starts` run to the exit rule; wall time, steps and the final
-    profile's difference from the empty-lattice run, which judges the others."""
+    profile's difference from the empty-lattice run, the reference result for the others."""
     assert starts[0] == "empty"
     R = sample_rates(n, count, np.random.default_rng(seed))
     rows = []
