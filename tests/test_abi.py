@@ -56,3 +56,18 @@ def test_no_device_reports_nodev():
         T.Meq(10)
     assert e.value.status == 4
     assert "no CUDA device" in str(e.value)
+
+
+def test_sweep_and_warm_start_entry_points_validate_arguments():
+    for n, nsys in ((11, 4), (25, 4), (16, 0)):
+        with pytest.raises(T.TasepError) as e:
+            T.Batch(n, nsys)
+        assert e.value.status == 1
+    L = T.lib()
+    assert L.tasep_mlp_create(0, 1, None) == 1
+    assert L.tasep_mlp_destroy(None) == 0
+    assert L.tasep_meq_init_pair_markov(None, None, None) == 1
+    hook_t = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, C.c_void_p)
+    L.tasep_meq_run_snapshots.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, hook_t, C.c_void_p, C.c_void_p]
+    assert L.tasep_meq_run_snapshots(None, None, 1, hook_t(lambda *a: None), None, None) == 1
+    assert b"" != L.tasep_last_error()
