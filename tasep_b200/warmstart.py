@@ -214,15 +214,18 @@ def predict_profile(mlp, rates):
     return rho, cov[: max(n - 1, 0)]
 
 
-STARTS = ("empty", "uniform", "meanfield", "pairfield", "learned")
+STARTS = ("empty", "uniform", "meanfield", "pairfield", "learned", "exactpair")
 
 
-def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, stop_tol=1e-10, device=-1):
+def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, stop_tol=1e-10, device=-1,
+                        profile=None):
     """Classical RK4 (FP64) from `start` to the exit rule: 'empty' (the
     empty lattice), 'uniform' (every state 2^-n), 'meanfield' (product
     measure of the mean-field profile), 'pairfield' (pair-Markov measure of
-    the pair approximation) or 'learned' (pair-Markov measure of the
-    network's prediction).  Returns (final state, run result, seconds
+    the pair approximation), 'learned' (pair-Markov measure of the network's
+    prediction) or 'exactpair' (pair-Markov measure of a given profile
+    (densities, nearest-neighbour covariances), e.g. the converged one: the
+    best any pair-Markov start can do).  Returns (final state, run result, seconds
     from the start's set-up - profile computation, network inference and
     measure construction included - to the end of the run, the start
     actually used)."""
@@ -243,6 +246,8 @@ def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, st
             init_pair_markov(m, mean_field_profile(rates), np.zeros(n - 1))
         elif start == "pairfield":
             init_pair_markov(m, *pair_field_profile(rates))
+        elif start == "exactpair":
+            init_pair_markov(m, profile[0], profile[1][: n - 1])
         elif start == "uniform":
             init_pair_markov(m, np.full(n, 0.5), np.zeros(n - 1))
         elif start == "empty":
@@ -275,7 +280,7 @@ def evaluate(mlp, n, count, seed=4, h=0.01, max_steps=2000000, starts=("empty", 
         row = {"n": n, "system": i}
         ref = None
         for s in starts:
-            x, res, sec, used = run_to_steady_state(n, r, s, mlp, h=h, max_steps=max_steps)
+            x, res, sec, used = run_to_steady_state(n, r, s, mlp, h=h, max_steps=max_steps, profile=ref)
             _, rho, cov = profile_targets(x, n)
             del x
             if ref is None:
