@@ -72,6 +72,17 @@ double me_win_corr(const me_obs *ob, int key, int offset);
 double me_win_error_guess(const me_obs *ob, int key, int offset);
 double me_win_closure(const me_obs *ob, int key, int offset);
 
+/* Learned warm start (--init learned): reads the shipped network parameters
+ * (a float32 .npy of TASEP_MLP_PARAMS values), builds the network inputs
+ * from the rates (first-order mean-field profile, 16 values per site),
+ * predicts on the GPU and sets the pair-Markov initial measure.  Returns 0,
+ * 1 if the prediction was infeasible (the handle is unchanged), -1 on error. */
+struct tasep_meq;
+int me_warm_params_load(const char *path, float *params);
+void me_warm_mean_field(int n, const double *rates, double *rho);
+void me_warm_features(int n, const double *rates, const double *mf, float *features);
+int me_warm_start(struct tasep_meq *m, int n, const double *rates, const char *params_path, int device);
+
 /* Minimal P6 writer (src/lib/graphlib.c:35-62 format). */
 typedef struct {
     unsigned char r, g, b;

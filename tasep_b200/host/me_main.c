@@ -11,7 +11,12 @@
  *   --integrator ref|rk4    ref (default): the reference's step bit for bit;
  *                           rk4: classical fourth-order Runge-Kutta
  *   --precision fp64|mixed  mixed: float stage vectors (rk4, constant rates)
- *   --init uniform|empty    initial state (default uniform, as the reference)
+ *   --init uniform|empty|learned
+ *                           initial state (default uniform, as the reference);
+ *                           learned: pair-Markov measure predicted by the
+ *                           shipped warm-start network (empty if infeasible)
+ *   --init-params <path>    network parameters for --init learned (default:
+ *                           data/warmstart_params.npy beside bin/)
  *   --init-file <path>      initial state from a probability file in this
  *                           program's output format
  *   --stop-tol <x>          exit when |dP|_1 < x*h (default 1e-10)
@@ -53,7 +58,9 @@ static void usage(const char *progname) {
            "--gamma <float> flow rate inside lattice\n"
            "--integrator <ref|rk4> step: the reference's (default) or classical RK4\n"
            "--precision <fp64|mixed> stage vectors in double (default) or float (rk4 only)\n"
-           "--init <uniform|empty> initial state (default uniform)\n"
+           "--init <uniform|empty|learned> initial state (default uniform); learned: warm start predicted by the "
+           "shipped network\n"
+           "--init-params <path> network parameters for --init learned\n"
            "--init-file <path> initial state from a probability file written by this program\n"
            "--stop-tol <float> exit when the L1 change per step stays below stop-tol*h (default 1e-10)\n"
            "--stop-count <int> ... for more than this many consecutive steps (default 100)\n"
@@ -65,8 +72,10 @@ static void usage(const char *progname) {
 enum {
     OPT_TIMEVAR = 0, OPT_FUNTYPE, OPT_OFFSET, OPT_AMPLITUDE, OPT_PERIOD, OPT_CONSTANT, OPT_SAVESEL, OPT_THREADS,
     OPT_ALPHA, OPT_BETA, OPT_GAMMA, OPT_INTEGRATOR, OPT_PRECISION, OPT_INIT, OPT_INITFILE, OPT_STOPTOL,
-    OPT_STOPCOUNT, OPT_DEVICE
+    OPT_STOPCOUNT, OPT_DEVICE, OPT_INITPARAMS
 };
+
+enum { ME_INIT_LEARNED = 100 };
 
 static struct option long_opt[] = {{"time-var", no_argument, NULL, OPT_TIMEVAR},
                                    {"function-type", required_argument, NULL, OPT_FUNTYPE},
@@ -86,6 +95,7 @@ static struct option long_opt[] = {{"time-var", no_argument, NULL, OPT_TIMEVAR},
                                    {"stop-tol", required_argument, NULL, OPT_STOPTOL},
                                    {"stop-count", required_argument, NULL, OPT_STOPCOUNT},
                                    {"device", required_argument, NULL, OPT_DEVICE},
+                                   {"init-params", required_argument, NULL, OPT_INITPARAMS},
                                    {NULL, 0, NULL, 0}};
 
 static void tasep_fail(const char *what) {
@@ -169,7 +179,7 @@ int main(int argc, char *argv[]) {
     long ncpu = sysconf(_SC_NPROCESSORS_ONLN);
     int num_threads = ncpu > 0 ? (int)ncpu : 1;
     int integrator = TASEP_INTEGRATOR_REF, precision = TASEP_PRECISION_FP64, init_kind = TASEP_INIT_UNIFORM;
-    char *init_file = NULL;
+    char *init_file = NULL, *init_params = NULL;
     double stop_condition = 1e-10;
     int stop_count = 100, device = -1;
     int err;
@@ -208,9 +218,11 @@ int main(int argc, char *argv[]) {
         case OPT_INIT:
             if (!strcmp(optarg, "uniform")) init_kind = TASEP_INIT_UNIFORM;
             else if (!strcmp(optarg, "empty")) init_kind = TASEP_INIT_EMPTY;
+            else if (!strcmp(optarg, "learned")) init_kind = ME_INIT_LEARNED;
             else { usage(argv[0]); exit(-1); }
             break;
         case OPT_INITFILE: init_file = strdup(optarg); break;
+        case OPT_INITPARAMS: init_params = strdup(optarg); break;
         case OPT_STOPTOL: stop_condition = atof(optarg); break;
         case OPT_STOPCOUNT: stop_count = atoi(optarg); break;
         case OPT_DEVICE: device = atoi(optarg); break;
@@ -278,6 +290,8 @@ int main(int argc, char *argv[]) {
     if (init_file) {
         if (read_prob_file(init_file, n, x) != 0) me_err_exit("ERROR: Could not read the initial state file", -1);
         printf("Read initial vector from '%s'\n", init_file);
+    } else if (init_kind == ME_INIT_LEARNED) {
+        printf("Initial vector from the learned warm start\n");
     } else if (init_kind == TASEP_INIT_EMPTY) {
         printf("Generated inital vector with empty lattice (P(0)=1)\n");
     } else {
@@ -422,6 +436,24 @@ int main(int argc, char *argv[]) {
         tasep_fail("time-variant rates");
     if (init_file) {
         if (tasep_meq_load(m, x) != TASEP_OK) tasep_fail("initial state");
+    } else if (init_kind == ME_INIT_LEARNED) {
+        char path[4096];
+        if (init_params) {
+            snprintf(path, sizeof path, "%s", init_params);
+        } else {  /* data/warmstart_params.npy beside the bin/ directory of this program */
+            ssize_t len = readlink("/proc/self/exe", path, sizeof path - 64);
+            if (len < 0) len = 0;
+            path[len] = 0;
+            char *slash = strrchr(path, '/');
+            if (slash) *slash = 0;
+            strcat(path, "/../data/warmstart_params.npy");
+        }
+        const int w = me_warm_start(m, n, rates, path, device);
+        if (w < 0) tasep_fail("learned warm start");
+        if (w == 1) {
+            printf("Warm-start prediction infeasible; starting from the empty lattice\n");
+            if (tasep_meq_init(m, TASEP_INIT_EMPTY) != TASEP_OK) tasep_fail("initial state");
+        }
     } else if (tasep_meq_init(m, init_kind) != TASEP_OK) {
         tasep_fail("initial state");
     }
@@ -549,5 +581,6 @@ int main(int argc, char *argv[]) {
     free(amplit_filename);
     free(constf_filename);
     free(init_file);
+    free(init_params);
     return 0;
 }

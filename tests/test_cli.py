@@ -175,6 +175,39 @@ def test_drop_in_rk4_empty_start_runs_to_the_exit_rule(tmp_path):
 
 
 @pytest.mark.gpu
+def test_drop_in_learned_warm_start(tmp_path):
+    """--init learned starts from the pair-Markov measure of the shipped
+    network's prediction (one step of h = 1e-30 leaves it as it was), the same
+    measure the Python driver builds, and runs to the cold start's steady state."""
+    from tasep_b200 import warmstart as ws
+    n = 12
+    r = ws.sample_rates(n, 1, np.random.default_rng(9))[0]
+    (tmp_path / "rates.txt").write_text(" ".join("%.17g" % v for v in r) + "\n")
+    p = run(["-n", str(n), "-i", "rates.txt", "-t", "0", "-T", "1e-30", "-s", "1", "--init", "learned",
+             "--save-select", "p", "-o", "w"], tmp_path)
+    assert p.returncode == 0, p.stderr
+    assert "Initial vector from the learned warm start" in p.stdout
+    x = np.zeros(1 << n)
+    for line in open(tmp_path / "w"):
+        b, v = line.split()
+        x[int(b, 2)] = float(v)
+    net = ws.pretrained()
+    rho, cov = ws.predict_profile(net, r)
+    net.close()
+    with T.Meq(n, T.INTEGRATOR_RK4) as m:
+        T.init_pair_markov(m, rho, cov)
+        ref = m.store()
+    assert np.max(np.abs(x - ref)) <= 1e-15
+    common = ["-n", str(n), "-i", "rates.txt", "-t", "0", "-T", "3000", "-s", "300000", "--integrator", "rk4",
+              "--save-select", "e"]
+    assert run(common + ["--init", "learned", "-o", "a"], tmp_path).returncode == 0
+    assert run(common + ["--init", "empty", "-o", "b"], tmp_path).returncode == 0
+    va = [float(v) for v in open(tmp_path / "a_exp_values_fin.vec").read().split(",")]
+    vb = [float(v) for v in open(tmp_path / "b_exp_values_fin.vec").read().split(",")]
+    assert max(abs(u - v) for u, v in zip(va, vb)) <= 2e-6  # printed with %lf
+
+
+@pytest.mark.gpu
 def test_drop_in_resume_from_probability_file(tmp_path):
     args = ["-n", "9", "--alpha", "0.3", "--beta", "0.8", "-t", "0", "-T", "5", "-s", "500", "--save-select", "p"]
     assert run(args + ["-o", "a"], tmp_path).returncode == 0

@@ -1,7 +1,9 @@
-"""Host side of the drop-in program without a GPU: the window observables and
-the snapshot writers of tasep_b200/host/me_output.c, compiled here into a
-small shared library, against the oracle's restatement of the reference
-functions (src/masterEquation.c:32-143, :1047-1110, :1516-1536)."""
+"""Host side of the drop-in program without a GPU, compiled here into small
+shared libraries: the window observables and the snapshot writers of
+tasep_b200/host/me_output.c against the oracle's restatement of the
+reference functions (src/masterEquation.c:32-143, :1047-1110, :1516-1536),
+and the warm-start inputs of tasep_b200/host/me_warm.c against the Python
+driver."""
 import ctypes as C
 import os
 import subprocess
@@ -31,7 +33,8 @@ class Snaps(C.Structure):
 def host(tmp_path_factory):
     out = tmp_path_factory.mktemp("host") / "libmeout.so"
     subprocess.run(["gcc", "-std=c99", "-O2", "-shared", "-fPIC", "-D_DEFAULT_SOURCE", "-pthread", "-I", HOST,
-                    os.path.join(HOST, "me_output.c"), "-lm", "-o", str(out)], check=True)
+                    "-I", os.path.join(ROOT, "include"), os.path.join(HOST, "me_output.c"), "-lm", "-o", str(out)],
+                   check=True)
     L = C.CDLL(str(out))
     dp = C.POINTER(C.c_double)
     L.me_state_corr.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int]
@@ -114,3 +117,35 @@ def test_snapshot_files_format(host, tmp_path):
     # without snapshots the probability file is empty, as the reference leaves it
     host.me_write_prb_txt(str(tmp_path / "e_prb.txt").encode(), None, 0.5)
     assert (tmp_path / "e_prb.txt").read_text() == ""
+
+
+@pytest.fixture(scope="module")
+def warm(tmp_path_factory):
+    import tasep_b200 as T
+    out = tmp_path_factory.mktemp("warm") / "libmewarm.so"
+    subprocess.run(["gcc", "-std=c99", "-O2", "-shared", "-fPIC", "-D_DEFAULT_SOURCE", "-I", HOST, "-I",
+                    os.path.join(ROOT, "include"), os.path.join(HOST, "me_warm.c"), "-L", os.path.dirname(T.LIB_PATH),
+                    "-ltasep_cuda", "-Wl,-rpath," + os.path.dirname(T.LIB_PATH), "-lm", "-o", str(out)], check=True)
+    L = C.CDLL(str(out))
+    L.me_warm_params_load.argtypes = [C.c_char_p, C.POINTER(C.c_float)]
+    L.me_warm_mean_field.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.me_warm_features.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_float)]
+    return L
+
+
+def test_drop_in_warm_start_inputs_match_the_python_driver(warm):
+    """--init learned builds the same network inputs as tasep_b200.warmstart and
+    reads the shipped parameters."""
+    from tasep_b200 import warmstart as ws
+    for n, seed in ((12, 1), (20, 2)):
+        r = ws.sample_rates(n, 1, np.random.default_rng(seed))[0]
+        mf = np.empty(n)
+        warm.me_warm_mean_field(n, _dp(r), _dp(mf))
+        assert np.array_equal(mf, ws.mean_field_profile(r))
+        f = np.empty((n, 16), dtype=np.float32)
+        warm.me_warm_features(n, _dp(r), _dp(mf), f.ctypes.data_as(C.POINTER(C.c_float)))
+        assert np.array_equal(f, ws.site_features(r))
+    p = np.empty(9538, dtype=np.float32)
+    assert warm.me_warm_params_load(ws.PRETRAINED.encode(), p.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    assert np.array_equal(p, np.load(ws.PRETRAINED))
+    assert warm.me_warm_params_load(b"/nonexistent.npy", p.ctypes.data_as(C.POINTER(C.c_float))) == -1
