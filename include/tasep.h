@@ -193,8 +193,9 @@ tasep_status tasep_batch_densities(tasep_batch *b, double *rho);
  * three hidden layers of 64 tanh units, 2 outputs: density and nearest-
  * neighbour covariance) trained on the GPU with the library's own forward
  * (tcgen05 tensor cores), backward and Adam kernels (BF16 weights, FP32
- * accumulation), and a device-
- * side builder of the pair-Markov initial measure from predicted profiles. */
+ * accumulation), and a device-side builder of the pair-Markov initial
+ * measure from predicted profiles.  A tensor-core wait that expires returns
+ * TASEP_ERR_TIMEOUT. */
 #define TASEP_MLP_IN 16
 #define TASEP_MLP_OUT 2
 #define TASEP_MLP_PARAMS 9538
