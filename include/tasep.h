@@ -155,6 +155,20 @@ tasep_status tasep_meq_observables(tasep_meq *m, double *rho, double *cov, doubl
 /* cudaStream_t the handle launches on. */
 void *tasep_meq_stream(const tasep_meq *m);
 
+/* L2 cache policy of the generator sweep (no counterpart in the reference,
+ * whose CSR product has no cache control).  A state's hop partners lie
+ * 2^k states ahead; the sweep reads a tile first as a partner of an earlier
+ * tile and last as its own tile.  near_bits: partner tiles of hops across
+ * the lowest near_bits tile-index bits are read with L2 evict_last (they come
+ * back as own tiles while L2 still holds them); farther partners follow
+ * TASEP_L2_FAR_FIRST.  flags: TASEP_L2_OWN_FIRST reads own tiles evict_first,
+ * TASEP_L2_DEMOTE lowers a tile's lines to evict_normal once its own read has
+ * landed, TASEP_L2_FAR_FIRST reads far partners evict_first.  Only speed
+ * depends on it, never the results; the default is the fastest measured. */
+enum { TASEP_L2_OWN_FIRST = 1, TASEP_L2_DEMOTE = 2, TASEP_L2_FAR_FIRST = 4 };
+tasep_status tasep_meq_set_cache_policy(tasep_meq *m, int near_bits, int flags);
+tasep_status tasep_meq_get_cache_policy(const tasep_meq *m, int *near_bits, int *flags);
+
 /* Per-kernel device time (CUDA events around each launch on the handle's
  * stream).  enable=1 starts recording and clears the totals. */
 tasep_status tasep_meq_profile(tasep_meq *m, int enable);
@@ -258,7 +272,10 @@ tasep_status tasep_step_ref_device(int n, const double *rates, double h, const d
  * (2^n doubles each, device memory, not overlapping), rates (n+1 doubles,
  * host memory) and checksum_dev (one double in device memory that receives the
  * step's L1 norm; NULL skips it).  Nothing is synchronised; results are ready
- * when `stream` reaches them.  All calls share the one array, and each call
+ * when `stream` reaches them.  The step's status stays in the shared array,
+ * so a bounded device wait that expired (TASEP_ERR_TIMEOUT for the other
+ * entry points) shows here as a NaN in *checksum_dev: pass checksum_dev to
+ * learn of it; x_out is then invalid.  All calls share the one array, and each call
  * clears its counter and status first, so calls that overlap on the GPU (on
  * different streams or from different threads without ordering) race and
  * must not be issued. */
@@ -267,6 +284,17 @@ tasep_status tasep_step_ref_device_noalloc(int n, const double *rates, double h,
 
 /* ---- misc ---------------------------------------------------------------- */
 const char *tasep_last_error(void);
+
+/* Test hook for the error path of the bounded device waits (no counterpart in
+ * the reference, which has no device code).  Every later launch of the
+ * generator sweep (n > 11) gives up a wait after wait_limit_ns (0 = the
+ * default, about 2 s) and, if skip_partner_copy >= 0, the first CTA leaves
+ * out that partner copy (counted from 0 within the launch), so a consumer
+ * wait on it expires.  The kernel then flags the error, lets the copies it
+ * did issue land and returns: no GPU fault, no hang.  Such steps report
+ * TASEP_ERR_TIMEOUT and their results are invalid.  (0, -1) switches the
+ * hook off; it is process-wide and not meant for concurrent use. */
+tasep_status tasep_test_inject_wait_expiry(uint64_t wait_limit_ns, int skip_partner_copy);
 int tasep_abi_version(void);
 /* Bytes of device memory a handle with this configuration allocates. */
 uint64_t tasep_meq_footprint(int n, int integrator, int precision, int timevar);

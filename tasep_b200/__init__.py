@@ -21,6 +21,7 @@ INCLUDE = os.path.join(os.path.dirname(PKG), "include", "tasep.h")
 INTEGRATOR_REF, INTEGRATOR_RK4 = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 INIT_UNIFORM, INIT_EMPTY = 0, 1
+L2_OWN_FIRST, L2_DEMOTE, L2_FAR_FIRST = 1, 2, 4
 FUN_SIN, FUN_COS, FUN_LIN = 0, 1, 2
 MAX_N = 33
 
@@ -37,6 +38,7 @@ EXPORTS = (
     "tasep_batch_init", "tasep_batch_load", "tasep_batch_run", "tasep_batch_store", "tasep_batch_densities",
     "tasep_mlp_create", "tasep_mlp_destroy", "tasep_mlp_set_params", "tasep_mlp_get_params", "tasep_mlp_loss_grad",
     "tasep_mlp_train", "tasep_mlp_predict", "tasep_meq_init_pair_markov", "tasep_meq_run_snapshots",
+    "tasep_meq_set_cache_policy", "tasep_meq_get_cache_policy", "tasep_test_inject_wait_expiry",
 )
 
 
@@ -101,6 +103,9 @@ def lib():
         L.tasep_abi_version.restype = C.c_int
         L.tasep_meq_footprint.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
         L.tasep_meq_footprint.restype = C.c_uint64
+        L.tasep_meq_set_cache_policy.argtypes = [H, C.c_int, C.c_int]
+        L.tasep_meq_get_cache_policy.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.tasep_test_inject_wait_expiry.argtypes = [C.c_uint64, C.c_int]
         _lib = L
     return _lib
 
@@ -112,6 +117,12 @@ def _check(st):
 
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def inject_wait_expiry(wait_limit_ns=0, skip_partner_copy=-1):
+    """Test hook: bounded device waits give up after wait_limit_ns and the first
+    CTA leaves out one partner copy (see include/tasep.h); (0, -1) turns it off."""
+    _check(lib().tasep_test_inject_wait_expiry(int(wait_limit_ns), int(skip_partner_copy)))
 
 
 def footprint(n, integrator=INTEGRATOR_RK4, precision=PRECISION_FP64, timevar=False):
@@ -225,6 +236,15 @@ class Meq:
 
     def profile(self, enable=True):
         _check(lib().tasep_meq_profile(self._h, int(enable)))
+
+    def set_cache_policy(self, near_bits, flags):
+        """L2 policy of the generator sweep (speed only; results do not depend on it)."""
+        _check(lib().tasep_meq_set_cache_policy(self._h, near_bits, flags))
+
+    def cache_policy(self):
+        a, b = C.c_int(0), C.c_int(0)
+        _check(lib().tasep_meq_get_cache_policy(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def profile_read(self):
         cap = 16

@@ -115,18 +115,19 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
     return t;
 }
 
-// Bounded wait: gives up after ~2 s (or as soon as another thread has
-// flagged an error), records the error and returns false.
+// Bounded wait: gives up after limit_ns (~2 s by default; or as soon as
+// another thread has flagged an error), records the error and returns false.
 constexpr uint64_t kWaitLimitNs = 2000000000ull;
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *err_flag) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *err_flag,
+                                          uint64_t limit_ns = kWaitLimitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_timer_ns();
     for (uint32_t it = 0;; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((it & 63) == 63) {
             if (*err_flag) return false;
-            if (global_timer_ns() - t0 > kWaitLimitNs) {
+            if (global_timer_ns() - t0 > limit_ns) {
                 *err_flag = 1;
                 return false;
             }
@@ -167,6 +168,12 @@ __device__ __forceinline__ uint64_t policy_evict_first() {
     uint64_t p;
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
     return p;
+}
+
+// Lowers the L2 eviction priority of one 128-byte line (if it is cached) to
+// evict_normal; a hint, no effect on the data.
+__device__ __forceinline__ void l2_demote_line(const void *p) {
+    asm volatile("applypriority.global.L2::evict_normal [%0], 128;" ::"l"(p) : "memory");
 }
 
 // Bulk global -> shared copy completing on an mbarrier (no multicast).

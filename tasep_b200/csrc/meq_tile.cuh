@@ -45,8 +45,24 @@ constexpr int kMaxRing = 16;                       // partner ring slots (upper 
 constexpr int kSmemMax = 232448;                   // dynamic shared memory per CTA on sm_100
 static_assert(kTile / 4 == kConsumers, "one group of four states per consumer thread");
 
+// L2 cache policy of the tile sweep (TileParams::l2_near, l2_flags).
+//
+// In the sweep order a tile is first read as a hop partner of an earlier tile
+// (T needs T + 2^u, 2^(u+1) tiles ahead) and last read as its own tile; after
+// that no later tile needs it (the entry partner, one tile later, excepted).
+// So the lines worth keeping are those of partner reads whose own read comes
+// within the L2 window: hop bits u < l2_near are read evict_last; the others
+// (partners whose own read is further away than L2 can hold) and, with
+// L2F_OWN_FIRST, the own-tile reads are evict_first, so they do not push the
+// useful lines out.  With L2F_DEMOTE the consumers lower the lines of a tile
+// they have just received to evict_normal, so a tile that was kept as a
+// partner stops occupying the evict_last class once it is no longer needed.
+enum : int { L2F_OWN_FIRST = 1, L2F_DEMOTE = 2, L2F_FAR_FIRST = 4 };
+
 struct TileParams {
     int n;
+    int l2_near;   // hop bits (tile-index bits) read evict_last as partners
+    int l2_flags;  // L2F_*
     unsigned long long ntiles;
     const void *g;             // gathered vector
     const void *s0, *s1, *s2;  // per-state extra inputs
@@ -61,6 +77,11 @@ struct TileParams {
     int stop_count;
     int exit_rule;
     int skip_if_done;
+    // Bounded waits: limit in ns (0 = kWaitLimitNs).  skip_copy_plus1 = k+1
+    // makes CTA 0's producer leave out its k-th partner copy, so the consumers'
+    // wait for it expires (tests of the error path; 0 = off).
+    unsigned long long wait_ns;
+    int skip_copy_plus1;
     RateSpec rs;
 };
 
@@ -195,23 +216,30 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     __syncthreads();
     if (c.skip) return;
     volatile int *errf = &c.err;
+    const uint64_t wait_ns = p.wait_ns ? p.wait_ns : kWaitLimitNs;
 
     const G *__restrict__ g = static_cast<const G *>(p.g);
 
     if (warp == kConsumerWarps) {
         // ---------------- producer ----------------
         if (lane == 0) {
-            const uint64_t keep = policy_evict_last();    // partner tiles: read again as self soon
+            const uint64_t keep = policy_evict_last();    // near partners: read again as own tile soon
             const uint64_t normal = policy_evict_normal();
+            const uint64_t first = policy_evict_first();
+            const uint64_t own_pol = (p.l2_flags & L2F_OWN_FIRST) ? first : normal;
+            const uint64_t far_pol = (p.l2_flags & L2F_FAR_FIRST) ? first : keep;
+            const uint64_t ent_pol = (p.l2_flags & L2F_DEMOTE) ? normal : keep;
+            const int near = p.l2_near;
+            const bool skip_copy = p.skip_copy_plus1 > 0 && blockIdx.x == 0;
             uint32_t it = 0, cur = 0;
             bool ok = true;
             for (unsigned long long ord = blockIdx.x; ord < p.ntiles && ok; ord += gridDim.x, ++it) {
                 const unsigned long long T = sweep_tile(ord, ntb);
                 const int b = it & 1;
-                if (it >= 2 && !mbar_wait(&c.empty[b], ((it >> 1) - 1) & 1, errf)) break;
+                if (it >= 2 && !mbar_wait(&c.empty[b], ((it >> 1) - 1) & 1, errf, wait_ns)) break;
                 unsigned char *st = stage_base + b * LY::stage;
                 mbar_arrive_expect_tx(&c.full[b], LY::stage);
-                bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], normal);  // read again only as a far partner
+                bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], own_pol);  // read again only as a far partner
                 // partner tiles, in the order the consumers add them
                 const bool top = (T >> (ntb - 1)) & 1;
                 const bool strad = !(T & 1);
@@ -222,8 +250,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 for (int q = 0; q < np; ++q) {
                     unsigned long long src;
                     uint32_t bytes = LY::gb;
+                    uint64_t pol = keep;
                     if (q == 0 && top) {
                         src = T - (1ull << (ntb - 1));
+                        pol = ent_pol;
                     } else if (q == int(top) && strad) {
                         src = T + 1;
                         bytes = LY::gb / 2;
@@ -231,14 +261,17 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                         const int u = __ffsll(hm) - 1;
                         hm &= hm - 1;
                         src = T + (1ull << u);
+                        if (u >= near) pol = far_pol;
                     }
                     const int slot = cur % RS;
-                    if (cur >= RS && !mbar_wait(&c.rempty[slot], ((cur / RS) - 1) & 1, errf)) {
+                    if (cur >= RS && !mbar_wait(&c.rempty[slot], ((cur / RS) - 1) & 1, errf, wait_ns)) {
                         ok = false;
                         break;
                     }
-                    mbar_arrive_expect_tx(&c.rfull[slot], bytes);
-                    bulk_g2s(ring_base + slot * LY::gb, g + src * kTile, bytes, &c.rfull[slot], keep);
+                    if (!(skip_copy && cur + 1 == uint32_t(p.skip_copy_plus1))) {
+                        mbar_arrive_expect_tx(&c.rfull[slot], bytes);
+                        bulk_g2s(ring_base + slot * LY::gb, g + src * kTile, bytes, &c.rfull[slot], pol);
+                    }
                     ++cur;
                 }
             }
@@ -281,6 +314,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     consumer_sync();
 
     const uint64_t once = policy_evict_first();
+    const bool demote = (p.l2_flags & L2F_DEMOTE) != 0;
     O *__restrict__ out = static_cast<O *>(p.out);
     const uint32_t t9 = tid;              // state bits 1..9
     const int pb0 = 2 * tid;              // local index of P0
@@ -344,7 +378,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         int eslot = 0;
         if (top) {  // 1. entry
             eslot = cslot;
-            if (!mbar_wait(&c.rfull[eslot], cph, errf)) { ok = false; break; }
+            if (!mbar_wait(&c.rfull[eslot], cph, errf, wait_ns)) { ok = false; break; }
             const G *ent = reinterpret_cast<const G *>(ring_base + eslot * LY::gb);
             G e0, e1, e2, e3;
             V2<G>::lds(ent + pb0, e0, e1);
@@ -353,8 +387,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             a2 = A::madd(a2, r0, e2); a3 = A::madd(a3, r0, e3);
             if (++cslot == RS) { cslot = 0; cph ^= 1; }  // released after the in-tile terms below
         }
-        if (!mbar_wait(&c.full[b], (it >> 1) & 1, errf)) { ok = false; break; }
+        if (!mbar_wait(&c.full[b], (it >> 1) & 1, errf, wait_ns)) { ok = false; break; }
         const G *xs = reinterpret_cast<const G *>(stage_base + b * LY::stage);
+        // this was the tile's last read of the sweep: its lines leave the evict_last class
+        if (demote && tid < LY::gb / 128) l2_demote_line(reinterpret_cast<const unsigned char *>(g + gT) + tid * 128);
 
         G x0, x1, x2, x3;
         V2<G>::lds(xs + pb0, x0, x1);
@@ -428,7 +464,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         }
         if (strad) {  // k = 10: P1 <- lower half of tile T+1
             const int slot = cslot;
-            if (!mbar_wait(&c.rfull[slot], cph, errf)) { ok = false; break; }
+            if (!mbar_wait(&c.rfull[slot], cph, errf, wait_ns)) { ok = false; break; }
             const G *hp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
             G p2, p3;
             V2<G>::lds(hp + pb0, p2, p3);
@@ -443,7 +479,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 const int u = __ffsll(mh) - 1;
                 mh &= mh - 1;
                 const int slot = cslot;
-                if (!mbar_wait(&c.rfull[slot], cph, errf)) { ok = false; break; }
+                if (!mbar_wait(&c.rfull[slot], cph, errf, wait_ns)) { ok = false; break; }
                 const G *pp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
                 const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 G p0, p1, p2, p3;
@@ -501,7 +537,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         V2<O>::stg(out + gT + pb1, o[2], o[3], once);
         consumer_release(&c.empty[b], lane);
     }
-    if (!ok || *errf) atomicExch(&p.ex->error, 1);
+    if (!ok || *errf) {
+        atomicExch(&p.ex->error, 1);
+        __threadfence();
+    }
 
     if constexpr (Tr::FINAL) {
         // deterministic CTA sum, then the last CTA reduces all partials in
@@ -525,7 +564,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             s = warp_sum(s);
             if (lane == 0) {
                 ExitState *ex = p.ex;
-                ex->last_checksum = s;
+                // a step with an expired wait has no valid norm: NaN marks it
+                // for callers that only read the norm (the status stays set)
+                const bool failed = *reinterpret_cast<volatile int *>(&ex->error) != 0;
+                ex->last_checksum = failed ? __longlong_as_double(0x7ff8000000000000ll) : s;
                 ex->steps_done = p.step + 1;
                 if (p.exit_rule) {
                     if (s < p.thresh) {

@@ -1,4 +1,5 @@
 // tasep_api.cu - C ABI of libtasep_cuda.so (declared in include/tasep.h).
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -73,13 +74,14 @@ tasep_status get_scratch(int dev, DevScratch **out) {
 }
 
 template <int S, typename E> tasep_status launch_tile(const TileParams &p, int grid, cudaStream_t st) {
-    static bool configured[64] = {};
+    // set once per device; concurrent first calls may both set it (idempotent)
+    static std::atomic<bool> configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     const int bytes = TileLayout<S, E>::bytes;
-    if (!configured[dev & 63]) {
+    if (!configured[dev & 63].load(std::memory_order_acquire)) {
         CU_TRY(cudaFuncSetAttribute(meq_tile_kernel<S, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        configured[dev & 63] = true;
+        configured[dev & 63].store(true, std::memory_order_release);
     }
     meq_tile_kernel<S, E><<<grid, kTileThreads, bytes, st>>>(p);
     CU_TRY(cudaGetLastError());
@@ -87,18 +89,32 @@ template <int S, typename E> tasep_status launch_tile(const TileParams &p, int g
 }
 
 template <typename E> tasep_status launch_small(const SmallParams &p, cudaStream_t st) {
-    static bool configured[64] = {};
+    static std::atomic<bool> configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     const size_t bytes = small_smem_bytes(p.n);
-    if (!configured[dev & 63]) {
+    if (!configured[dev & 63].load(std::memory_order_acquire)) {
         CU_TRY(cudaFuncSetAttribute(meq_small_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(small_smem_bytes(kSmallMaxN))));
-        configured[dev & 63] = true;
+        configured[dev & 63].store(true, std::memory_order_release);
     }
     meq_small_kernel<E><<<1, kSmallThreads, bytes, st>>>(p);
     CU_TRY(cudaGetLastError());
     return TASEP_OK;
+}
+
+// Default L2 policy of the tile sweep (L2F_* in meq_tile.cuh).
+int g_l2_near_default = 64;
+int g_l2_flags_default = 0;
+
+// tasep_test_inject_wait_expiry: wait limit and left-out partner copy of
+// every tile launch (0 = off).
+std::atomic<unsigned long long> g_test_wait_ns{0};
+std::atomic<int> g_test_skip_copy{0};
+
+void apply_test_hook(TileParams &p) {
+    p.wait_ns = g_test_wait_ns.load();
+    p.skip_copy_plus1 = g_test_skip_copy.load();
 }
 
 void fill_const_rates(RateSpec &rs, int n, const double *r) {
@@ -124,6 +140,7 @@ struct tasep_meq {
     double *obs_part = nullptr, *obs_out = nullptr;
     int obs_rows = 0;
     int cur = 0;
+    int l2_near = 64, l2_flags = 0;  // L2 policy of the tile sweep
     bool rates_set = false, state_set = false;
     RateSpec rs{};
     // profiling
@@ -181,6 +198,9 @@ TileParams base_params(tasep_meq *m, double h, unsigned long long step, double t
     TileParams p;
     memset(&p, 0, sizeof p);
     p.n = m->n;
+    p.l2_near = m->l2_near;
+    p.l2_flags = m->l2_flags;
+    apply_test_hook(p);
     p.ntiles = m->ntiles;
     p.h = h;
     p.partials = m->partials;
@@ -271,6 +291,13 @@ bool valid_handle(const tasep_meq *m) { return m != nullptr && m->n >= 1; }
 extern "C" {
 
 const char *tasep_last_error(void) { return g_last_error.c_str(); }
+
+tasep_status tasep_test_inject_wait_expiry(uint64_t wait_limit_ns, int skip_partner_copy) {
+    if (skip_partner_copy < -1) return fail(TASEP_ERR_INVALID, "skip_partner_copy %d < -1", skip_partner_copy);
+    g_test_wait_ns.store(wait_limit_ns);
+    g_test_skip_copy.store(skip_partner_copy + 1);
+    return TASEP_OK;
+}
 int tasep_abi_version(void) { return TASEP_ABI_VERSION; }
 
 uint64_t tasep_meq_footprint(int n, int integrator, int precision, int timevar) {
@@ -306,6 +333,8 @@ tasep_status tasep_meq_create(const tasep_meq_config *cfg, tasep_meq **out) {
     m->precision = cfg->precision;
     m->device = dev;
     m->N = 1ull << cfg->n;
+    m->l2_near = g_l2_near_default;
+    m->l2_flags = g_l2_flags_default;
     m->ntiles = cfg->n > kSmallMaxN ? (m->N >> kTileBits) : 1;
     cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
     m->grid = int(m->ntiles < (unsigned long long)m->nsm ? m->ntiles : m->nsm);
@@ -610,11 +639,11 @@ tasep_status tasep_meq_observables(tasep_meq *m, double *rho, double *cov, doubl
     if (!m->state_set) return fail(TASEP_ERR_INVALID, "initial state not set");
     CU_TRY(cudaSetDevice(m->device));
     const int n = m->n, na = obs_count(n);
-    static bool configured[64] = {};
-    if (!configured[m->device & 63]) {
+    static std::atomic<bool> configured[64] = {};
+    if (!configured[m->device & 63].load(std::memory_order_acquire)) {
         CU_TRY(cudaFuncSetAttribute(meq_obs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(obs_smem_bytes(TASEP_MAX_N))));
-        configured[m->device & 63] = true;
+        configured[m->device & 63].store(true, std::memory_order_release);
     }
     ObsParams op{n, m->X[m->cur], m->obs_part};
     tasep_status s = prof_begin(m, ST_COUNT + 1);
@@ -651,6 +680,22 @@ tasep_status tasep_meq_observables(tasep_meq *m, double *rho, double *cov, doubl
 }
 
 void *tasep_meq_stream(const tasep_meq *m) { return m ? static_cast<void *>(m->stream) : nullptr; }
+
+tasep_status tasep_meq_set_cache_policy(tasep_meq *m, int near_bits, int flags) {
+    if (!valid_handle(m)) return fail(TASEP_ERR_INVALID, "null handle");
+    if (near_bits < 0 || near_bits > 64 || (flags & ~(TASEP_L2_OWN_FIRST | TASEP_L2_DEMOTE | TASEP_L2_FAR_FIRST)))
+        return fail(TASEP_ERR_INVALID, "cache policy near_bits=%d flags=%d out of range", near_bits, flags);
+    m->l2_near = near_bits;
+    m->l2_flags = flags;
+    return TASEP_OK;
+}
+
+tasep_status tasep_meq_get_cache_policy(const tasep_meq *m, int *near_bits, int *flags) {
+    if (!valid_handle(m)) return fail(TASEP_ERR_INVALID, "null handle");
+    if (near_bits) *near_bits = m->l2_near;
+    if (flags) *flags = m->l2_flags;
+    return TASEP_OK;
+}
 
 tasep_status tasep_meq_profile(tasep_meq *m, int enable) {
     if (!valid_handle(m)) return fail(TASEP_ERR_INVALID, "null handle");
@@ -709,6 +754,9 @@ tasep_status tasep_apply_device(int n, const double *rates, const double *x, dou
     TileParams p;
     memset(&p, 0, sizeof p);
     p.n = n;
+    p.l2_near = g_l2_near_default;
+    p.l2_flags = g_l2_flags_default;
+    apply_test_hook(p);
     p.ntiles = (1ull << n) >> kTileBits;
     p.g = x;
     p.out = y;
@@ -748,6 +796,9 @@ tasep_status tasep_step_ref_device(int n, const double *rates, double h, const d
         TileParams p;
         memset(&p, 0, sizeof p);
         p.n = n;
+        p.l2_near = g_l2_near_default;
+        p.l2_flags = g_l2_flags_default;
+        apply_test_hook(p);
         p.ntiles = (1ull << n) >> kTileBits;
         p.g = x;
         p.out = x_out;
@@ -841,6 +892,9 @@ extern "C" tasep_status tasep_step_ref_device_noalloc(int n, const double *rates
         TileParams p;
         memset(&p, 0, sizeof p);
         p.n = n;
+        p.l2_near = g_l2_near_default;
+        p.l2_flags = g_l2_flags_default;
+        apply_test_hook(p);
         p.ntiles = ntiles;
         p.g = x;
         p.out = x_out;

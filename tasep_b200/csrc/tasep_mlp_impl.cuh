@@ -30,14 +30,14 @@ uint64_t mlp_rng(uint64_t &s) {  // splitmix64
 double mlp_unif(uint64_t &s) { return double(mlp_rng(s) >> 11) * (1.0 / 9007199254740992.0); }
 
 tasep_status mlp_configure() {
-    static bool done[64] = {};
+    static std::atomic<bool> done[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    if (!done[dev & 63]) {
+    if (!done[dev & 63].load(std::memory_order_acquire)) {
         CU_TRY(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     int(kMlpForwardSmem)));
         CU_TRY(cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kMlpGradSmem)));
-        done[dev & 63] = true;
+        done[dev & 63].store(true, std::memory_order_release);
     }
     return TASEP_OK;
 }

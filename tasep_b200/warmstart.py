@@ -36,6 +36,7 @@ import time
 import numpy as np
 
 from . import Batch, INIT_EMPTY, INTEGRATOR_RK4, Meq, Mlp, PRECISION_FP64, TasepError, init_pair_markov
+from . import closure
 
 COV_SCALE = 10.0
 MF_STEPS = 20000
@@ -214,7 +215,15 @@ def predict_profile(mlp, rates):
     return rho, cov[: max(n - 1, 0)]
 
 
-STARTS = ("empty", "uniform", "meanfield", "pairfield", "learned", "exactpair")
+STARTS = ("empty", "uniform", "meanfield", "pairfield", "closure3", "closure4", "learned", "exactpair")
+CLOSURE_TOL = 1e-7  # window change rate at which the closure hierarchy counts as stationary
+
+
+def closure_start_profile(rates, order):
+    """Densities and nearest-neighbour covariances of the steady state of the
+    mean-field closure hierarchy of order `order` (tasep_b200/closure.py, the
+    reference's src/mf_full.c model) for one rate vector or a batch."""
+    return closure.steady_profile(rates, order, tol=CLOSURE_TOL)
 
 
 def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, stop_tol=1e-10, device=-1,
@@ -225,7 +234,9 @@ def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, st
     the pair approximation), 'learned' (pair-Markov measure of the network's
     prediction) or 'exactpair' (pair-Markov measure of a given profile
     (densities, nearest-neighbour covariances), e.g. the converged one: the
-    best any pair-Markov start can do).  Returns (final state, run result, seconds
+    best any pair-Markov start can do), 'closure3' / 'closure4' (pair-Markov
+    measure of the steady state of the mean-field closure hierarchy of that
+    order; `profile` may hold it precomputed).  Returns (final state, run result, seconds
     from the start's set-up - profile computation, network inference and
     measure construction included - to the end of the run, the start
     actually used)."""
@@ -246,6 +257,11 @@ def run_to_steady_state(n, rates, start, mlp=None, h=0.01, max_steps=2000000, st
             init_pair_markov(m, mean_field_profile(rates), np.zeros(n - 1))
         elif start == "pairfield":
             init_pair_markov(m, *pair_field_profile(rates))
+        elif start in ("closure3", "closure4"):
+            if profile is not None:  # computed ahead for a whole set (batched), time added by the caller
+                init_pair_markov(m, profile[0], profile[1][: n - 1])
+            else:
+                init_pair_markov(m, *closure_start_profile(rates, int(start[-1])))
         elif start == "exactpair":
             init_pair_markov(m, profile[0], profile[1][: n - 1])
         elif start == "uniform":
@@ -275,12 +291,22 @@ def evaluate(mlp, n, count, seed=4, h=0.01, max_steps=2000000, starts=("empty", 
     profile's difference from the empty-lattice run, the reference result for the others."""
     assert starts[0] == "empty"
     R = sample_rates(n, count, np.random.default_rng(seed))
+    # closure profiles of the whole set in one batched host computation; each
+    # system's start is charged its share of that time
+    cl_prof, cl_sec = {}, {}
+    for s in starts:
+        if s in ("closure3", "closure4"):
+            t0 = time.perf_counter()
+            cl_prof[s] = closure_start_profile(R, int(s[-1]))
+            cl_sec[s] = (time.perf_counter() - t0) / len(R)
     rows = []
     for i, r in enumerate(R):
         row = {"n": n, "system": i}
         ref = None
         for s in starts:
-            x, res, sec, used = run_to_steady_state(n, r, s, mlp, h=h, max_steps=max_steps, profile=ref)
+            prof = (cl_prof[s][0][i], cl_prof[s][1][i]) if s in cl_prof else ref
+            x, res, sec, used = run_to_steady_state(n, r, s, mlp, h=h, max_steps=max_steps, profile=prof)
+            sec += cl_sec.get(s, 0.0)
             _, rho, cov = profile_targets(x, n)
             del x
             if ref is None:
@@ -294,6 +320,8 @@ def evaluate(mlp, n, count, seed=4, h=0.01, max_steps=2000000, starts=("empty", 
         row["prediction_cov_err"] = float(np.abs(cov_p - ref[1][: n - 1]).max())
         row["meanfield_density_err"] = float(np.abs(mean_field_profile(r) - ref[0]).max())
         row["pairfield_density_err"] = float(np.abs(pair_field_profile(r)[0] - ref[0]).max())
+        for s in cl_prof:
+            row[f"{s}_density_err"] = float(np.abs(cl_prof[s][0][i] - ref[0]).max())
         for s in starts[1:]:
             row[s]["speedup"] = round(row["empty"]["seconds"] / row[s]["seconds"], 3)
         rows.append(row)
@@ -311,6 +339,9 @@ def summarize(rows, starts=("empty", "meanfield", "learned")):
              "prediction_density_err_median": float(np.median([r["prediction_density_err"] for r in rs])),
              "meanfield_density_err_median": float(np.median([r["meanfield_density_err"] for r in rs])),
              "pairfield_density_err_median": float(np.median([r["pairfield_density_err"] for r in rs]))}
+        for st in ("closure3", "closure4"):
+            if f"{st}_density_err" in rs[0]:
+                s[f"{st}_density_err_median"] = float(np.median([r[f"{st}_density_err"] for r in rs]))
         for st in starts[1:]:
             tw = sum(r[st]["seconds"] for r in rs)
             s[st] = {"seconds": round(tw, 3), "wall_time_ratio": round(tc / tw, 3),

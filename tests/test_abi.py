@@ -71,3 +71,13 @@ def test_sweep_and_warm_start_entry_points_validate_arguments():
     L.tasep_meq_run_snapshots.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, hook_t, C.c_void_p, C.c_void_p]
     assert L.tasep_meq_run_snapshots(None, None, 1, hook_t(lambda *a: None), None, None) == 1
     assert b"" != L.tasep_last_error()
+
+
+def test_cache_policy_and_test_hook_validate_without_a_device():
+    L = T.lib()
+    assert L.tasep_meq_set_cache_policy(None, 12, 0) == 1
+    assert L.tasep_meq_get_cache_policy(None, None, None) == 1
+    with pytest.raises(T.TasepError) as e:
+        T.inject_wait_expiry(0, -2)
+    assert e.value.status == 1
+    T.inject_wait_expiry(0, -1)  # off: accepted without a device

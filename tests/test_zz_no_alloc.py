@@ -43,3 +43,30 @@ def test_noalloc_step_matches_allocating_step(n):
         torch.cuda.synchronize()
         assert torch.equal(out, ref_out)
         assert cs.item() == ref_cs
+
+
+def test_noalloc_step_marks_an_expired_wait_with_nan():
+    """The allocation-free step keeps its status in the shared static array,
+    out of the caller's reach; a bounded wait that expired must still be
+    visible, as a NaN norm in checksum_dev.  The next call, with the test hook
+    off, must clear that state and agree with the allocating step again."""
+    import torch
+    assert torch.cuda.is_available(), "CUDA device required"
+    n = 14
+    r = rates_for(n, 61)
+    x = torch.from_numpy(np.random.default_rng(61).random(1 << n)).cuda()
+    out = torch.empty_like(x)
+    cs = torch.zeros(1, dtype=torch.float64, device="cuda")
+    try:
+        T.inject_wait_expiry(1_000_000, 0)
+        T.step_ref_device_noalloc(n, r, 0.01, x.data_ptr(), out.data_ptr(), cs.data_ptr())
+        torch.cuda.synchronize()
+    finally:
+        T.inject_wait_expiry(0, -1)
+    assert np.isnan(cs.item())
+    ref_out = torch.empty_like(x)
+    ref_cs = T.step_ref_device(n, r, 0.01, x.data_ptr(), ref_out.data_ptr())
+    T.step_ref_device_noalloc(n, r, 0.01, x.data_ptr(), out.data_ptr(), cs.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref_out)
+    assert cs.item() == ref_cs
