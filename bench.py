@@ -19,9 +19,11 @@ timed region.
 
 reference: the reference's own CPU step (src/lib/solv.c rk4_step x4 + the
 serial update of src/masterEquation.c:639-642), compiled from the reference
-sources into oracle/_ref, timed on the host cores with all threads on a
-bounded row sample of the same n=28 generator; steps/s are scaled from the
-sample to all 2^28 rows.
+sources into oracle/_ref, timed on the host cores with all threads over all
+2^28 rows of the n=28 generator (CSR of about 52 GB, built untimed) when the
+host has the memory, else on a bounded row sample scaled to all rows and
+marked "extrapolated".  The line records the host's CPU model, core count and
+memory.
 """
 from __future__ import annotations
 
@@ -149,6 +151,33 @@ def replicas_value(world, steps, ms):
     return world * steps / (ms / 1000.0)
 
 
+def host_info():
+    """CPU model, logical cores and memory of this host (for the CPU baseline)."""
+    info = {"cpu_model": None, "logical_cpus": os.cpu_count(), "mem_total_gb": None, "mem_available_gb": None}
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    info["cpu_model"] = line.split(":", 1)[1].strip()
+                    break
+        with open("/proc/meminfo") as f:
+            for line in f:
+                k, v = line.split(":", 1)
+                if k in ("MemTotal", "MemAvailable"):
+                    info["mem_total_gb" if k == "MemTotal" else "mem_available_gb"] = round(
+                        int(v.split()[0]) / 1048576.0, 1)
+    except OSError:
+        pass
+    return info
+
+
+def reference_full_bytes(n):
+    """Host memory of the reference's -f step on all rows: CSR + 6 vectors."""
+    dim = 1 << n
+    nnz = 2 * dim + (dim >> 2) * (n - 1)
+    return 8 * (dim + 1) + 16 * nnz + 6 * 8 * dim
+
+
 def cpu_baseline_sample(n, rates, h, target_s=15.0):
     """Reference -f step on a row sample; returns (steps/s scaled to all rows, info)."""
     import oracle as O
@@ -168,7 +197,8 @@ def cpu_baseline_sample(n, rates, h, target_s=15.0):
     value = (rows / float(1 << n)) / secs
     return value, {"cores": threads, "sample": f"reference rk4_step x4 + serial update over rows "
                    f"[0, 2^{int(np.log2(rows))}) of the 2^{n}-state generator ({nnz} CSR entries), "
-                   f"{reps} timed steps of {secs:.3f} s each, scaled to all rows"}
+                   f"{reps} timed steps of {secs:.3f} s each, scaled to all rows (a bounded sample; "
+                   f"bench.py --impl reference times all rows)", "host": host_info()}
 
 
 def run_reference(args):
@@ -188,17 +218,35 @@ def run_reference(args):
         print(json.dumps(line))
         return 0
     threads = O.ref().refh_max_threads()
-    rows = 1 << min(n, 22)
-    s1, _ = O.ref_time_sample(n, rows, rates, 0.01, reps=1, nthreads=threads)
-    per_step_budget = 60.0 / max(args.steps + 1, 1)
-    rows = min(1 << n, 1 << 25, max(1 << 20, int(rows * per_step_budget / max(s1, 1e-3))))
-    rows = 1 << int(np.log2(rows))
-    secs, nnz = O.ref_time_sample(n, rows, rates, 0.01, reps=args.steps, nthreads=threads)
-    value = (rows / float(1 << n)) / secs
-    line.update({"value": value, "ms_per_step": 1000.0 / value,
-                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                                  "sample": f"rows [0, 2^{int(np.log2(rows))}) of 2^{n} ({nnz} CSR entries), "
-                                            f"{args.steps} timed steps after 1 untimed, scaled to all rows"},
+    host = host_info()
+    need = reference_full_bytes(n)
+    avail = (host["mem_available_gb"] or 0.0) * 1073741824.0
+    if avail >= 1.15 * need:
+        # the whole generator: every one of the 2^n rows, as the reference runs it
+        warm = min(args.warmup, 2)
+        secs, build, nnz = O.ref_time_full(n, rates, 0.01, warm=warm, reps=args.steps, nthreads=threads)
+        if secs > 0:
+            value = 1.0 / secs
+            cb = {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "extrapolated": False,
+                  "sample": f"all 2^{n} rows ({nnz} CSR entries, {need / 1e9:.1f} GB), {args.steps} timed "
+                            f"steps after {warm} untimed; CSR set-up {build:.1f} s (untimed)",
+                  "host": host}
+    else:
+        secs = -1.0
+    if secs <= 0:
+        rows = 1 << min(n, 22)
+        s1, _ = O.ref_time_sample(n, rows, rates, 0.01, reps=1, nthreads=threads)
+        per_step_budget = 60.0 / max(args.steps + 1, 1)
+        rows = min(1 << n, 1 << 25, max(1 << 20, int(rows * per_step_budget / max(s1, 1e-3))))
+        rows = 1 << int(np.log2(rows))
+        secs, nnz = O.ref_time_sample(n, rows, rates, 0.01, reps=args.steps, nthreads=threads)
+        value = (rows / float(1 << n)) / secs
+        cb = {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "extrapolated": True,
+              "sample": f"rows [0, 2^{int(np.log2(rows))}) of 2^{n} ({nnz} CSR entries), {args.steps} timed "
+                        f"steps after 1 untimed, scaled to all rows: the whole generator needs "
+                        f"{need / 1e9:.1f} GB of host memory, {host['mem_available_gb']} GB available",
+              "host": host}
+    line.update({"value": value, "ms_per_step": 1000.0 / value, "cpu_baseline": cb,
                  "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     print(json.dumps(line))
     return 0
@@ -218,6 +266,7 @@ def run_ours(args):
     m = T.Meq(n, integ, prec, device=local)
     m.set_rates(rates)
     m.init(T.INIT_EMPTY)
+    policy = m.cache_policy()
     stream = torch.cuda.ExternalStream(m.stream)
 
     def barrier():
@@ -273,18 +322,25 @@ def run_ours(args):
         avg = tot_ms / cnt
         b = ALG_BYTES.get((name, prec), 0) * N
         achieved = b / (avg / 1000.0) / 1e9
-        traffic = None
+        # DRAM traffic is not measured in this run (that needs ncu): it comes from
+        # the stored capture of the same kernel, workload size and cache policy
+        traffic, traffic_src = None, None
         tp = os.path.join(ROOT, "profiles", "ncu_traffic.json")
         if os.path.exists(tp):
             with open(tp) as f:
                 tr = json.load(f)
             k = f"{name}/{args.precision}"
-            if k in tr and tr[k].get("n") == n:  # measured on this workload size only
-                traffic = tr[k]["bytes_per_state"] * N
+            rec = tr.get(k, {})
+            if rec.get("n") == n and rec.get("l2_policy") == list(policy):
+                traffic = rec["bytes_per_state"] * N
+                traffic_src = f"stored ncu capture ({rec.get('source', 'profiles/ncu_traffic.json')}), not this run"
+        kernel_ms = {k: v[0] / v[1] for k, v in prof.items()}
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                "alg_bytes_per_launch": b, "avg_launch_ms": avg,
-                "kernel_ms": {k: v[0] / v[1] for k, v in prof.items()}}
+                "traffic_source": traffic_src, "alg_bytes_per_launch": b, "avg_launch_ms": avg,
+                "kernel_ms": kernel_ms,
+                "kernel_frac": {k: ALG_BYTES.get((k, prec), 0) * N / (v / 1000.0) / 1e9 / peak
+                                for k, v in kernel_ms.items()}}
     launches = int(sum(v[1] for v in prof.values()))
     step_alg = STEP_BYTES.get((integ, prec), 0) * N
     cpu = None
@@ -292,7 +348,7 @@ def run_ours(args):
         cb = cpu_baseline_sample(n, rates, h)
         if cb is not None:
             cpu = {"value": cb[0], "unit": UNIT, "cores": cb[1]["cores"], "kind": "reference",
-                   "sample": cb[1]["sample"]}
+                   "extrapolated": True, "sample": cb[1]["sample"], "host": cb[1]["host"]}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -301,6 +357,7 @@ def run_ours(args):
                                f"{'classical RK4' if integ else 'reference step'}",
                    "n": n, "integrator": args.integrator, "precision": args.precision,
                    "replicas": world, "l2": "inputs larger than L2 (8*2^n bytes per vector)",
+                   "l2_policy": {"near_bits": policy[0], "flags": policy[1]},
                    "hbm_step_bytes_algorithmic": step_alg,
                    "step_hbm_gbs_algorithmic": step_alg / (ms / args.steps / 1000.0) / 1e9},
         "roofline": roof, "cpu_baseline": cpu,

@@ -252,6 +252,24 @@ def ref_run(n, rates, h=0.01, steps=100, init=INIT_EMPTY, stop_tol=1e-10, stop_c
     return x, res.as_dict()
 
 
+def ref_csr_matches_gencrs(n, rates):
+    """True when the harness's parallel CSR builder reproduces gencrs exactly."""
+    L = ref()
+    L.refh_csr_matches_gencrs.argtypes = [C.c_int, _dp]
+    return L.refh_csr_matches_gencrs(n, _d(_f64(rates))) == 1
+
+
+def ref_time_full(n, rates, h=0.01, warm=1, reps=1, nthreads=0):
+    """Seconds per reference -f step over all 2^n rows, set-up seconds and nnz."""
+    L = ref()
+    L.refh_time_full.argtypes = [C.c_int, _dp, C.c_double, C.c_int, C.c_int, C.c_int, _dp,
+                                 C.POINTER(C.c_uint64)]
+    L.refh_time_full.restype = C.c_double
+    build, nnz = C.c_double(0.0), C.c_uint64(0)
+    s = L.refh_time_full(n, _d(_f64(rates)), h, warm, reps, nthreads, C.byref(build), C.byref(nnz))
+    return s, float(build.value), int(nnz.value)
+
+
 def ref_time_sample(n, rows, rates, h=0.01, reps=1, nthreads=0):
     """Seconds per reference -f step over the first `rows` rows (and nnz)."""
     nnz = C.c_uint64(0)

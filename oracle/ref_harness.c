@@ -234,4 +234,94 @@ double refh_time_sample(int n, uint64_t rows, const double *rates, double h, int
     return secs;
 }
 
+/* The -f generator built row by row in parallel with the reference's own
+ * gen_meq_row (src/lib/solv.c:81-135), which yields the rows gencrs writes
+ * (src/lib/matgen.c:29-67; refh_csr_matches_gencrs checks it).  The serial
+ * gencrs, with its progress line per row, takes minutes at n = 28. */
+static void build_csr_parallel(int n, uint64_t rows, double *rates, uint64_t *rowPtr, double *valArr,
+                               uint64_t *colInd)
+{
+    const uint64_t hopmask = RH_POW2(n - 1) - 1;
+    uint64_t acc = 0;
+    for (uint64_t i = 0; i < rows; i++) {
+        rowPtr[i] = acc;
+        acc += 1 + ((i >> (n - 1)) & 1) + !(i & 1) + (uint64_t)__builtin_popcountll(i & ~(i >> 1) & hopmask);
+    }
+    rowPtr[rows] = acc;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)rows; i++)
+        gen_meq_row(n, (uint_fast64_t)i, rates, valArr + rowPtr[i], (uint_fast64_t *)(colInd + rowPtr[i]));
+}
+
+/* 1 if the parallel builder reproduces gencrs's CSR exactly (n <= 20). */
+int refh_csr_matches_gencrs(int n, const double *rates_in)
+{
+    if (n < 2 || n > 20) return -1;
+    const uint64_t dim = RH_POW2(n), size = 2 * RH_POW2(n) + RH_POW2(n - 2) * (n - 1);
+    double r[72];
+    memcpy(r, rates_in, (size_t)(n + 1) * sizeof(double));
+    uint64_t *p1 = malloc((dim + 1) * sizeof(uint64_t)), *p2 = malloc((dim + 1) * sizeof(uint64_t));
+    uint64_t *c1 = malloc(size * sizeof(uint64_t)), *c2 = malloc(size * sizeof(uint64_t));
+    double *v1 = malloc(size * sizeof(double)), *v2 = malloc(size * sizeof(double));
+    int ok = p1 && p2 && c1 && c2 && v1 && v2;
+    if (ok) {
+        build_csr(n, dim, r, p1, v1, c1);
+        build_csr_parallel(n, dim, r, p2, v2, c2);
+        ok = !memcmp(p1, p2, (dim + 1) * sizeof(uint64_t)) && p1[dim] == size &&
+             !memcmp(c1, c2, size * sizeof(uint64_t)) && !memcmp(v1, v2, size * sizeof(double));
+    }
+    free(p1); free(p2); free(c1); free(c2); free(v1); free(v2);
+    return ok;
+}
+
+/*
+ * The reference's -f step on the WHOLE 2^n-state generator (the bench's
+ * reference arm): CSR of all rows (built in parallel, above), x uniform, then
+ * `warm` untimed and `reps` timed steps of rk4_step x4 + the serial update and
+ * L1 norm (src/masterEquation.c:628-642).  Returns seconds per step, or a
+ * negative value when memory runs out; *build_secs gets the set-up time.
+ */
+double refh_time_full(int n, const double *rates, double h, int warm, int reps, int nthreads,
+                      double *build_secs, uint64_t *nnz_out)
+{
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+    const uint64_t dim = RH_POW2(n);
+    const uint64_t size = 2 * RH_POW2(n) + RH_POW2(n - 2) * (n - 1);
+    const double tb = now_s();
+    uint64_t *rowPtr = malloc((dim + 1) * sizeof(uint64_t));
+    double *valArr = malloc(size * sizeof(double));
+    uint64_t *colInd = malloc(size * sizeof(uint64_t));
+    double *x = malloc(dim * sizeof(double)), *x1 = malloc(dim * sizeof(double));
+    double *k1 = malloc(dim * sizeof(double)), *k2 = malloc(dim * sizeof(double));
+    double *k3 = malloc(dim * sizeof(double)), *k4 = malloc(dim * sizeof(double));
+    double secs = -1.0;
+    if (rowPtr && valArr && colInd && x && x1 && k1 && k2 && k3 && k4) {
+        double r[72];
+        memcpy(r, rates, (size_t)(n + 1) * sizeof(double));
+        build_csr_parallel(n, dim, r, rowPtr, valArr, colInd);
+        if (nnz_out) *nnz_out = rowPtr[dim];
+#pragma omp parallel for schedule(static)
+        for (uint64_t i = 0; i < dim; i++) x[i] = 1.0 / (double)dim;
+        if (build_secs) *build_secs = now_s() - tb;
+        double t0 = 0, checksum = 0;
+        for (int rep = -warm; rep < reps; rep++) {
+            if (rep == 0) t0 = now_s();
+            checksum = 0;
+            rk4_step(1, dim, k1, x, x1, rowPtr, colInd, valArr, h);
+            rk4_step(2, dim, k2, x, x1, rowPtr, colInd, valArr, h);
+            rk4_step(3, dim, k3, x, x1, rowPtr, colInd, valArr, h);
+            rk4_step(4, dim, k4, x, x1, rowPtr, colInd, valArr, h);
+            for (uint64_t k = 0; k < dim; k++) {
+                x[k] += (k1[k] + (2. * k2[k]) + (2. * k3[k]) + k4[k]) / 6.;
+                checksum += fabs((k1[k] + (2. * k2[k]) + (2. * k3[k]) + k4[k]) / 6.);
+            }
+        }
+        secs = (now_s() - t0) / (reps > 0 ? reps : 1);
+        if (!(checksum >= 0)) secs = -2.0;
+    }
+    free(rowPtr); free(valArr); free(colInd); free(x); free(x1);
+    free(k1); free(k2); free(k3); free(k4);
+    return secs;
+}
+
 int refh_max_threads(void) { return omp_get_max_threads(); }

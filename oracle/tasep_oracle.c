@@ -57,6 +57,55 @@ static double row_sum(int n, uint64_t i, const double *r, const double *x)
     return t;
 }
 
+/* The generator as CSR, built once per run for constant rates: the reference's
+ * -f path (gencrs, src/lib/matgen.c:7-74, then the CSR gather of
+ * src/lib/solv.c:9-13).  Rows hold the same entries in the same order as
+ * orc_gen_row, so every row sum is bit-identical to row_sum; the CSR only
+ * saves regenerating the rows at every stage. */
+typedef struct {
+    uint64_t *rowptr, *col;
+    double *val;
+} orc_csr;
+
+static int csr_build(int n, const double *r, orc_csr *m)
+{
+    const int64_t dim = (int64_t)ORC_POW2(n);
+    const uint64_t nnz = 2 * (uint64_t)dim + (uint64_t)(n - 1) * ((uint64_t)dim >> 2); /* src/masterEquation.c:593 */
+    m->rowptr = (uint64_t *)malloc(((size_t)dim + 1) * sizeof(uint64_t));
+    m->col = (uint64_t *)malloc(((size_t)nnz + 1) * sizeof(uint64_t));
+    m->val = (double *)malloc(((size_t)nnz + 1) * sizeof(double));
+    if (!m->rowptr || !m->col || !m->val) {
+        free(m->rowptr); free(m->col); free(m->val);
+        return -1;
+    }
+    const uint64_t hopmask = ORC_POW2(n - 1) - 1;
+    uint64_t acc = 0;
+    for (int64_t i = 0; i < dim; i++) {  /* row lengths: diagonal, entry, exit, active hops */
+        const uint64_t u = (uint64_t)i;
+        m->rowptr[i] = acc;
+        acc += 1 + ((u >> (n - 1)) & 1) + !(u & 1) + (uint64_t)__builtin_popcountll(u & ~(u >> 1) & hopmask);
+    }
+    m->rowptr[dim] = acc;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < dim; i++) orc_gen_row(n, (uint64_t)i, r, m->val + m->rowptr[i], m->col + m->rowptr[i]);
+    return 0;
+}
+
+static void csr_free(orc_csr *m)
+{
+    free(m->rowptr); free(m->col); free(m->val);
+}
+
+static double csr_row(const orc_csr *m, uint64_t i, const double *x)
+{
+    double t = 0.0;
+    for (uint64_t j = m->rowptr[i]; j < m->rowptr[i + 1]; j++) t += m->val[j] * x[m->col[j]];
+    return t;
+}
+
+/* row i of M x: from the CSR when there is one, else generated on the fly */
+#define ROW(csr, n, i, r, x) ((csr) ? csr_row((csr), (i), (x)) : row_sum((n), (i), (r), (x)))
+
 void orc_apply(int n, const double *r, const double *x, double *y)
 {
     const int64_t dim = (int64_t)ORC_POW2(n);
@@ -90,11 +139,11 @@ void orc_timevar_rates(int count, const double *period, const double *offset,
 }
 
 /* src/masterEquation.c:628-642 with src/lib/solv.c:3-26. */
-double orc_step_ref(int n, const double *r, double h, double *x, double *k)
+static double step_ref(int n, const double *r, const orc_csr *csr, double h, double *x, double *k)
 {
     const int64_t dim = (int64_t)ORC_POW2(n);
 #pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < dim; i++) k[i] = h * row_sum(n, (uint64_t)i, r, x);
+    for (int64_t i = 0; i < dim; i++) k[i] = h * ROW(csr, n, (uint64_t)i, r, x);
     double checksum = 0;
     for (int64_t i = 0; i < dim; i++) {
         /* k1 = k2 = k3 = k4 = k[i] */
@@ -105,34 +154,39 @@ double orc_step_ref(int n, const double *r, double h, double *x, double *k)
     return checksum;
 }
 
+double orc_step_ref(int n, const double *r, double h, double *x, double *k)
+{
+    return step_ref(n, r, NULL, h, x, k);
+}
+
 /* Classical RK4 with the stage vector of src/lib/solv.c:14-24 fed back as the
- * gather input of the next stage. */
-double orc_step_rk4(int n, const double *r1, const double *r2, const double *r3,
-                    const double *r4, double h, double *x, double *s)
+ * gather input of the next stage (csr: the constant-rate generator, or NULL). */
+static double step_rk4(int n, const double *r1, const double *r2, const double *r3, const double *r4,
+                       const orc_csr *csr, double h, double *x, double *s)
 {
     const int64_t dim = (int64_t)ORC_POW2(n);
     double *k1 = s, *k2 = s + dim, *k3 = s + 2 * dim, *k4 = s + 3 * dim;
     double *u = s + 4 * dim, *v = s + 5 * dim;
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < dim; i++) {
-        double t = row_sum(n, (uint64_t)i, r1, x);
+        double t = ROW(csr, n, (uint64_t)i, r1, x);
         k1[i] = h * t;
         u[i] = (0.5 * h * t) + x[i];
     }
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < dim; i++) {
-        double t = row_sum(n, (uint64_t)i, r2, u);
+        double t = ROW(csr, n, (uint64_t)i, r2, u);
         k2[i] = h * t;
         v[i] = (0.5 * h * t) + x[i];
     }
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < dim; i++) {
-        double t = row_sum(n, (uint64_t)i, r3, v);
+        double t = ROW(csr, n, (uint64_t)i, r3, v);
         k3[i] = h * t;
         u[i] = (h * t) + x[i];
     }
 #pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < dim; i++) k4[i] = h * row_sum(n, (uint64_t)i, r4, u);
+    for (int64_t i = 0; i < dim; i++) k4[i] = h * ROW(csr, n, (uint64_t)i, r4, u);
     double checksum = 0;
     for (int64_t i = 0; i < dim; i++) {
         double d = (k1[i] + (2. * k2[i]) + (2. * k3[i]) + k4[i]) / 6.;
@@ -141,6 +195,15 @@ double orc_step_rk4(int n, const double *r1, const double *r2, const double *r3,
     }
     return checksum;
 }
+
+double orc_step_rk4(int n, const double *r1, const double *r2, const double *r3,
+                    const double *r4, double h, double *x, double *s)
+{
+    return step_rk4(n, r1, r2, r3, r4, NULL, h, x, s);
+}
+
+/* Largest n whose constant-rate runs keep the generator as CSR (about 0.5 GB). */
+#define ORC_CSR_MAX_N 22
 
 /* src/masterEquation.c:402-409 (uniform start), :586 (h), :628-682 (loop and
  * exit rule), :883-897 (time-var: rates at the step start, no exit test). */
@@ -160,6 +223,9 @@ int orc_run(const orc_run_cfg *c, double *x, orc_run_result *res)
     }
     double *scratch = (double *)malloc((c->integrator == ORC_INT_RK4 ? 6 : 1) * dim * sizeof(double));
     if (!scratch) return -1;
+    orc_csr csr_store, *csr = NULL;
+    if (!c->timevar && n <= ORC_CSR_MAX_N && c->steps > 1 && csr_build(n, c->rates, &csr_store) == 0)
+        csr = &csr_store;
     double ra[4][72];
     double t = c->t0, h = c->h, cs = 0;
     int early_stop = 0;
@@ -176,9 +242,9 @@ int orc_run(const orc_run_cfg *c, double *x, orc_run_result *res)
             for (int s = 0; s < 4; s++) memcpy(ra[s], c->rates, (size_t)(n + 1) * sizeof(double));
         }
         if (c->integrator == ORC_INT_RK4)
-            cs = orc_step_rk4(n, ra[0], ra[1], ra[2], ra[3], h, x, scratch);
+            cs = step_rk4(n, ra[0], ra[1], ra[2], ra[3], csr, h, x, scratch);
         else
-            cs = orc_step_ref(n, ra[0], h, x, scratch);
+            cs = step_ref(n, ra[0], csr, h, x, scratch);
         t += h;
         if (c->exit_rule) {
             if (cs < c->stop_tol * h) {
@@ -194,6 +260,7 @@ int orc_run(const orc_run_cfg *c, double *x, orc_run_result *res)
         }
     }
     free(scratch);
+    if (csr) csr_free(csr);
     res->steps_done = i;
     res->steps_at_stop = steps_at_stop;
     res->early_stop = early_stop;

@@ -330,6 +330,96 @@ def evaluate(mlp, n, count, seed=4, h=0.01, max_steps=2000000, starts=("empty", 
     return rows
 
 
+def start_profiles(mlp, R, start, ref_profiles=None):
+    """Per-system (densities, nearest-neighbour covariances) of a start for a
+    batch of rate vectors R, or None for the empty lattice."""
+    n = R.shape[1] - 1
+    if start == "empty":
+        return None
+    if start == "meanfield":
+        return [(mean_field_profile(r), np.zeros(n - 1)) for r in R]
+    if start == "pairfield":
+        rho, cov = pair_field_profile(R)
+        return list(zip(rho, cov))
+    if start in ("closure3", "closure4"):
+        rho, cov = closure_start_profile(R, int(start[-1]))
+        return list(zip(rho, cov))
+    if start == "learned":
+        return [predict_profile(mlp, r) for r in R]
+    if start == "exactpair":
+        return [(p[0], p[1][: n - 1]) for p in ref_profiles]
+    raise ValueError(f"unknown start {start!r}")
+
+
+def evaluate_batched(mlp, n, count, seed=4, h=0.01, max_steps=4000000, stop_tol=1e-10,
+                     starts=("empty", "learned"), device=-1, log=None):
+    """The held-out evaluation with all `count` systems of a start in one batch
+    (tasep_batch_*), so that 64 vectors at n = 24 fit a GPU session: per system,
+    the steps to its exit rule from each start, whose ratio to the empty
+    lattice's is the wall-time ratio of single-system runs (every step of a
+    system costs the same); the final profile's difference from the
+    empty-lattice run; the batch's own wall time.  Starts other than the empty
+    lattice are built per system on the device (pair-Markov measure) and loaded
+    into the batch; an infeasible profile falls back to the empty lattice."""
+    assert starts[0] == "empty"
+    R = sample_rates(n, count, np.random.default_rng(seed))
+    N = 1 << n
+    out = {"n": n, "systems": count, "seed": seed, "h": h, "stop_tol": stop_tol, "starts": {}}
+    ref_prof = None
+    for st in starts:
+        t0 = time.perf_counter()
+        prof = start_profiles(mlp, R, st, ref_prof)
+        t_prof = time.perf_counter() - t0
+        with Batch(n, count, PRECISION_FP64, device=device) as b:
+            b.set_rates(R)
+            used = [st] * count
+            t1 = time.perf_counter()
+            if prof is None:
+                b.init(INIT_EMPTY)
+            else:
+                X = np.empty((count, N))
+                m = Meq(n, INTEGRATOR_RK4, PRECISION_FP64, device=device)
+                try:
+                    for s in range(count):
+                        m.set_rates(R[s])
+                        try:
+                            init_pair_markov(m, prof[s][0], prof[s][1])
+                        except TasepError:
+                            m.init(INIT_EMPTY)
+                            used[s] = "empty (fallback)"
+                        m.store(X[s])
+                finally:
+                    m.close()
+                b.load(X)
+                del X
+            t_init = time.perf_counter() - t1
+            t2 = time.perf_counter()
+            res, sched = b.run(h, max_steps, stop_tol=stop_tol)
+            t_run = time.perf_counter() - t2
+            finals = [profile_targets(b.store(s), n)[1:] for s in range(count)]
+        if st == "empty":
+            ref_prof = finals
+        rec = {"profile_seconds": round(t_prof, 3), "init_seconds": round(t_init, 3),
+               "run_seconds": round(t_run, 3), "schedule": sched,
+               "steps": [int(r["steps_done"]) for r in res], "converged": [bool(r["converged"]) for r in res],
+               "fallbacks": sum(u != st for u in used),
+               "max_density_diff": [float(np.abs(f[0] - rf[0]).max()) for f, rf in zip(finals, ref_prof)],
+               "max_cov_diff": [float(np.abs(f[1] - rf[1]).max()) for f, rf in zip(finals, ref_prof)]}
+        if prof is not None:
+            rec["start_density_err"] = [float(np.abs(p[0] - rf[0]).max()) for p, rf in zip(prof, ref_prof)]
+        if st != "empty":
+            e = np.array(out["starts"]["empty"]["steps"], dtype=float)
+            w = np.array(rec["steps"], dtype=float)
+            ratio = e / w
+            rec["step_ratio_total"] = round(float(e.sum() / w.sum()), 4)
+            rec["step_ratio_median"] = round(float(np.median(ratio)), 4)
+            rec["step_ratio_min_max"] = [round(float(ratio.min()), 4), round(float(ratio.max()), 4)]
+        out["starts"][st] = rec
+        if log:
+            log({"n": n, "start": st, **{k: v for k, v in rec.items() if not isinstance(v, list)}})
+    return out
+
+
 def summarize(rows, starts=("empty", "meanfield", "learned")):
     out = {}
     for n in sorted({r["n"] for r in rows}):
@@ -370,6 +460,8 @@ def main(argv=None):
     ap.add_argument("--epochs", type=float, default=1.0, help="scale of the default training schedule")
     ap.add_argument("--starts", default="empty,meanfield,learned", help="starts to compare (empty first)")
     ap.add_argument("--out", default=None, help="JSON report")
+    ap.add_argument("--batched", action="store_true",
+                    help="evaluate each start's held-out systems in one batch (steps to the exit rule per system)")
     a = ap.parse_args(argv)
     starts = tuple(a.starts.split(","))
 
@@ -377,6 +469,16 @@ def main(argv=None):
         print(json.dumps(rec), flush=True)
 
     report = {}
+    if a.batched:  # evaluation of the shipped (or given) network only
+        mlp = Mlp(seed=0)
+        mlp.params = np.load(a.params if a.params else PRETRAINED)
+        report["eval_batched"] = [evaluate_batched(mlp, n, count, starts=starts, log=log)
+                                  for n, count in _pairs(a.eval)]
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(report, f, indent=1)
+        mlp.close()
+        return
     if a.params and os.path.exists(a.params) and not a.data:  # evaluation of a trained network only
         mlp = Mlp(seed=0)
         mlp.params = np.load(a.params)

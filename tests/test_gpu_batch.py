@@ -71,3 +71,55 @@ def test_batch_mixed_precision_densities():
     for s in range(nsys):
         xo, _ = O.run(n, R[s], h=0.01, steps=400000, integrator=O.INT_RK4, init=O.INIT_EMPTY, stop_tol=1e-10)
         assert np.max(np.abs(rho[s] - O.densities(n, xo))) <= 1e-6
+
+
+# The standard sweep (1024 systems, n = 16, (alpha, beta) grid, seed-2 hops):
+# a 32-system slice spread over the grid.
+SLICE = [32 * a + b for a in (4, 9, 14, 19) for b in (4, 7, 10, 13, 16, 19, 22, 25)]
+
+
+def test_sweep_slice_fixed_steps_matches_oracle():
+    """32 systems of the standard n = 16 sweep, 300 RK4 steps: every system
+    within 1e-12 of the oracle's single-system run."""
+    from tasep_b200.sweep import sweep_rates
+    R = sweep_rates()[SLICE]
+    n, steps = 16, 300
+    with T.Batch(n, len(SLICE)) as b:
+        b.set_rates(R)
+        b.init(T.INIT_EMPTY)
+        res, _ = b.run(0.01, steps, exit_rule=False)
+        finals = [b.store(s) for s in range(len(SLICE))]
+    for s in range(len(SLICE)):
+        xo, _ = O.run(n, R[s], h=0.01, steps=steps, integrator=O.INT_RK4, init=O.INIT_EMPTY, exit_rule=False)
+        assert res[s]["steps_done"] == steps
+        assert np.max(np.abs(finals[s] - xo)) <= 1e-12
+
+
+def test_sweep_slice_each_system_to_its_own_exit_rule():
+    """The same 32 systems under the exit rule: each retires on its own step,
+    equal (within the rounding-level slack of the other exit tests) to the
+    single-system integrator's run of that rate vector, with the state within
+    1e-12; two of them also against the oracle's own run to the exit rule."""
+    from tasep_b200.sweep import sweep_rates
+    R = sweep_rates()[SLICE]
+    n, tol, cap = 16, 1e-8, 400000
+    with T.Batch(n, len(SLICE)) as b:
+        b.set_rates(R)
+        b.init(T.INIT_EMPTY)
+        res, _ = b.run(0.01, cap, stop_tol=tol)
+        finals = [b.store(s) for s in range(len(SLICE))]
+    steps = [r["steps_done"] for r in res]
+    assert all(r["converged"] == 1 for r in res)
+    assert len(set(steps)) > 8  # systems retire at different steps
+    for s in range(len(SLICE)):
+        with T.Meq(n, T.INTEGRATOR_RK4) as m:
+            m.set_rates(R[s])
+            m.init(T.INIT_EMPTY)
+            rs = m.run(0.01, cap, stop_tol=tol)
+            x = m.store()
+        assert abs(int(rs["steps_done"]) - int(steps[s])) <= 2
+        assert np.max(np.abs(finals[s] - x)) <= 1e-12
+    for s in sorted(range(len(SLICE)), key=lambda k: steps[k])[:2]:
+        xo, ro = O.run(n, R[s], h=0.01, steps=cap, integrator=O.INT_RK4, init=O.INIT_EMPTY, stop_tol=tol)
+        assert abs(int(ro["steps_done"]) - int(steps[s])) <= 2
+        assert np.max(np.abs(finals[s] - xo)) <= 1e-12

@@ -279,7 +279,7 @@ def test_mass_conservation_n24(integrator, precision):
     assert abs(x.sum() - 1.0) < 1e-12
 
 
-@pytest.mark.parametrize("n,integrator", [(26, O.INT_RK4), (26, O.INT_REF), (28, O.INT_RK4)])
+@pytest.mark.parametrize("n,integrator", [(26, O.INT_RK4), (26, O.INT_REF), (28, O.INT_RK4), (28, O.INT_REF)])
 def test_steps_random_dense_state_full_size(n, integrator):
     """A random dense state at n=26 and at the benchmark size n=28 (up to 131072
     tiles, every shared-memory buffer reused hundreds of times per launch): each
@@ -343,3 +343,43 @@ def test_run_snapshots_stop_at_the_exit_rule(n):
     assert res == res2 and res["converged"] == 1
     last = res["steps_done"] - 1
     assert steps == list(range(0, last + 1, 7))
+
+
+def test_timevar_rk4_many_tiles_per_cta():
+    """Time-variant classical RK4 (stage kernels U1..U4, rates evaluated on the
+    device at t, t+h/2, t+h/2, t+h) at n=23: 4096 tiles, every partner ring slot
+    reused many times per launch; within 1e-12 of the oracle."""
+    n = 23
+    rng = np.random.default_rng(23)
+    base = rates_for(n, 1)
+    tv = {"type": np.zeros(n + 1, dtype=np.int32), "amplitude": 0.5 * base,
+          "period": rng.uniform(0.5, 2, n + 1), "offset": np.zeros(n + 1), "constant": base}
+    x0 = rng.random(1 << n)
+    x0 /= x0.sum()
+    steps = 4
+    xo, _ = O.run(n, base, h=0.01, steps=steps, integrator=O.INT_RK4, x0=x0, timevar=tv, exit_rule=False)
+    with T.Meq(n, T.INTEGRATOR_RK4) as m:
+        m.set_rates(base)
+        m.set_timevar(tv["type"], tv["amplitude"], tv["period"], tv["offset"], tv["constant"])
+        m.load(x0)
+        res = m.run(0.01, steps, exit_rule=False)
+        x = m.store()
+    assert res["steps_done"] == steps
+    assert np.max(np.abs(x - xo)) <= PROB_TOL, _mismatch_report(x, xo)
+
+
+@pytest.mark.parametrize("n", [22, 24])
+def test_mixed_precision_against_fp64_many_tiles(n):
+    """FP32 stage vectors against the FP64 integrator on the same lattice
+    (2^22 and 2^24 states, many tiles per CTA): densities within 1e-6 and
+    total probability within 1e-8 after 3000 steps from the empty lattice."""
+    r = rates_for(n, 2)
+    out = {}
+    for prec in (T.PRECISION_FP64, T.PRECISION_MIXED):
+        with T.Meq(n, T.INTEGRATOR_RK4, prec) as m:
+            m.set_rates(r)
+            m.init(T.INIT_EMPTY)
+            m.run(0.01, 3000, exit_rule=False)
+            out[prec] = m.observables()
+    assert np.max(np.abs(out[T.PRECISION_MIXED]["rho"] - out[T.PRECISION_FP64]["rho"])) <= 1e-6
+    assert abs(out[T.PRECISION_MIXED]["mass"] - 1.0) <= 1e-8
