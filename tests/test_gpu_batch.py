@@ -123,3 +123,21 @@ def test_sweep_slice_each_system_to_its_own_exit_rule():
         xo, ro = O.run(n, R[s], h=0.01, steps=cap, integrator=O.INT_RK4, init=O.INIT_EMPTY, stop_tol=tol)
         assert abs(int(ro["steps_done"]) - int(steps[s])) <= 2
         assert np.max(np.abs(finals[s] - xo)) <= 1e-12
+
+
+def test_autotuner_picks_a_valid_schedule_and_changes_no_result():
+    """schedule=-1: the autotuner times the schedules and reports the one it
+    kept; results equal those of a fixed schedule bit for bit (a schedule only
+    decides which CTA sweeps which tile)."""
+    n, nsys, steps = 13, 6, 200
+    R = sweep_rates(n, nsys, 4)
+    out = {}
+    for sched in (-1, 0, 1):
+        with T.Batch(n, nsys) as b:
+            b.set_rates(R)
+            b.init(T.INIT_EMPTY)
+            res, used = b.run(0.01, steps, exit_rule=False, schedule=sched)
+            out[sched] = (used, [b.store(s) for s in range(nsys)])
+    assert out[-1][0] in (0, 1)
+    for s in range(nsys):
+        assert np.array_equal(out[-1][1][s], out[out[-1][0]][1][s])
