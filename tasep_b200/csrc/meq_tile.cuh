@@ -24,8 +24,8 @@
 //     staged tile with predicated loads (fully unrolled, so independent chains
 //     interleave); high hops read the ring slots in ascending bit order.  The
 //     diagonal's low part (everything up to bit 9, which precedes the tile-
-//     level terms in the reference's subtraction order) is computed once per
-//     launch into registers, the remaining terms are subtracted in order, so
+//     level terms in the reference's subtraction order) comes from a table
+//     built once per launch, the remaining terms are subtracted in order, so
 //     the reference's rounding sequence is kept exactly.
 // All CTAs sweep the tiles together (natural order, except that the entry bit
 // toggles fastest: sweep_tile), so partner tiles up to a few tens of MB ahead
@@ -146,11 +146,7 @@ template <int S, typename E> struct TileLayout {
     static constexpr int x1b = Tr::NX > 1 ? kTile * sizeof(typename Tr::X1) : 0;
     static constexpr int x2b = Tr::NX > 2 ? kTile * sizeof(typename Tr::X2) : 0;
     static constexpr int stage = gb;     // the gathered tile; extras go straight to registers
-    // The low diagonal prefixes live in registers, except for the exact
-    // stages with per-state extra inputs (time-variant RK4), whose registers
-    // are taken by the extras: those keep a table in shared memory.
-    static constexpr bool diag_regs = !Tr::EXACT || Tr::NX == 0;
-    static constexpr int dtab = diag_regs ? 0 : 2 * gb;  // table for top bit clear / set
+    static constexpr int dtab = 2 * gb;  // low diagonal prefixes, for top bit clear / set
     // as many partner slots as shared memory holds
     static constexpr int RS0 = (kSmemMax - kCtrlBytes - 2 * stage - dtab) / gb;
     static constexpr int RS = RS0 < kMaxRing ? RS0 : kMaxRing;
@@ -191,7 +187,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     TileCtrl &c = *reinterpret_cast<TileCtrl *>(tile_smem);
     unsigned char *stage_base = tile_smem + kCtrlBytes;
     unsigned char *ring_base = stage_base + 2 * LY::stage;
-    G *dtab = reinterpret_cast<G *>(ring_base + LY::RS * LY::gb);  // used when !LY::diag_regs
+    G *dtab = reinterpret_cast<G *>(ring_base + LY::RS * LY::gb);
     constexpr int RS = LY::RS;
 
     const int tid = threadIdx.x;
@@ -303,32 +299,19 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     //
     // Low diagonal prefixes: d = 0; -r[n] if b0; -r[0] if top clear; then
     // -r[n-1-j] for j = 0..9 where b_j = 0, b_(j+1) = 1 (src/lib/solv.c:103-116).
-    // Kept in registers for the thread's four states (top set: dl1; top clear:
-    // dl0, or dl1 - r[0] where the stage may reassociate), else in a table.
-    auto low_prefix = [&](int l, int tp) {
-        G d = G(0);
-        if (l & 1) d = A::sub(d, rate_of<G>(c, n));
-        if (!tp) d = A::sub(d, rate_of<G>(c, 0));
-        for (int j = 0; j < kTileBits - 1; ++j)
-            if (!((l >> j) & 1) && ((l >> (j + 1)) & 1)) d = A::sub(d, rate_of<G>(c, n - 1 - j));
-        return d;
-    };
-    constexpr bool kDl0 = LY::diag_regs && Tr::EXACT;
-    G dl0[kDl0 ? 4 : 1], dl1[4];
-    if constexpr (LY::diag_regs) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int l = 2 * tid + (q & 1) + (q >> 1) * (kTile / 2);
-            dl1[q] = low_prefix(l, 1);
-            if constexpr (kDl0) dl0[q] = low_prefix(l, 0);
+    for (int l = tid; l < kTile; l += kConsumers) {
+        for (int tp = 0; tp < 2; ++tp) {
+            G d = G(0);
+            if (l & 1) d = A::sub(d, rate_of<G>(c, n));
+            if (!tp) d = A::sub(d, rate_of<G>(c, 0));
+            for (int j = 0; j < kTileBits - 1; ++j)
+                if (!((l >> j) & 1) && ((l >> (j + 1)) & 1)) d = A::sub(d, rate_of<G>(c, n - 1 - j));
+            dtab[tp * kTile + l] = d;
         }
-    } else {
-        for (int l = tid; l < kTile; l += kConsumers)
-            for (int tp = 0; tp < 2; ++tp) dtab[tp * kTile + l] = low_prefix(l, tp);
-        consumer_sync();
     }
     const G rn = rate_of<G>(c, n), r0 = rate_of<G>(c, 0), rn1 = rate_of<G>(c, n - 1);
     const G r9 = rate_of<G>(c, n - 10), rnL = rate_of<G>(c, n - kTileBits);
+    consumer_sync();
 
     const uint64_t once = policy_evict_first();
     const bool demote = (p.l2_flags & L2F_DEMOTE) != 0;
@@ -412,19 +395,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         G x0, x1, x2, x3;
         V2<G>::lds(xs + pb0, x0, x1);
         V2<G>::lds(xs + pb1, x2, x3);
-        // 2. diagonal: low prefix, then j = 10 and j >= 11
+        // 2. diagonal: low prefix from the table, then j = 10 and j >= 11
+        const G *dt = dtab + (top ? kTile : 0);
         G d0, d1, d2, d3;
-        if constexpr (!LY::diag_regs) {
-            const G *dt = dtab + (top ? kTile : 0);
-            V2<G>::lds(dt + pb0, d0, d1);
-            V2<G>::lds(dt + pb1, d2, d3);
-        } else if constexpr (kDl0) {
-            d0 = top ? dl1[0] : dl0[0]; d1 = top ? dl1[1] : dl0[1];
-            d2 = top ? dl1[2] : dl0[2]; d3 = top ? dl1[3] : dl0[3];
-        } else {
-            const G e = top ? G(0) : r0;
-            d0 = dl1[0] - e; d1 = dl1[1] - e; d2 = dl1[2] - e; d3 = dl1[3] - e;
-        }
+        V2<G>::lds(dt + pb0, d0, d1);
+        V2<G>::lds(dt + pb1, d2, d3);
         if (!strad) {  // j = 10: b10 = 0 (P0), b11 = 1
             d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL);
         }
