@@ -193,11 +193,20 @@ tasep_status tasep_batch_set_rates(tasep_batch *b, const double *rates);
 tasep_status tasep_batch_init(tasep_batch *b, int kind);
 /* host_x: nsys*2^n doubles. */
 tasep_status tasep_batch_load(tasep_batch *b, const double *host_x);
-/* res: nsys results (NULL skips them).  schedule: -1 = choose by timing,
- * 0 = interleaved, 1 = system per SM; *schedule_used (may be NULL) reports
- * the choice. */
+/* res: nsys results (NULL skips them).  schedule: -1 = choose, 0 = tiles
+ * interleaved over the SMs, 1 = whole systems per SM, 2 = cluster-resident:
+ * each system held entirely in the shared memory of one thread-block cluster
+ * (2^(n-13) .. 2^(n-11) CTAs, n <= 17) and run to its exit rule there, with no
+ * device-memory traffic between steps.  -1 takes 2 when n <= 17 (timing its
+ * shapes on a short run of copies of the first systems and keeping the
+ * fastest), else times 0 and 1.  *schedule_used (may be NULL) reports the
+ * choice. */
 tasep_status tasep_batch_run(tasep_batch *b, const tasep_run_config *rc, int schedule, tasep_run_result *res,
                              int *schedule_used);
+/* The configuration the last tasep_batch_run used: schedule, states per CTA
+ * and CTAs per system (0 for schedules 0 and 1). */
+tasep_status tasep_batch_last_config(const tasep_batch *b, int *schedule, int *states_per_cta,
+                                     int *ctas_per_system);
 tasep_status tasep_batch_store(const tasep_batch *b, int sys, double *host_x);
 /* Per-bit densities of every system: nsys*n doubles (bit order). */
 tasep_status tasep_batch_densities(tasep_batch *b, double *rho);

@@ -39,6 +39,7 @@ EXPORTS = (
     "tasep_mlp_create", "tasep_mlp_destroy", "tasep_mlp_set_params", "tasep_mlp_get_params", "tasep_mlp_loss_grad",
     "tasep_mlp_train", "tasep_mlp_predict", "tasep_meq_init_pair_markov", "tasep_meq_run_snapshots",
     "tasep_meq_set_cache_policy", "tasep_meq_get_cache_policy", "tasep_test_inject_wait_expiry",
+    "tasep_batch_last_config",
 )
 
 
@@ -271,6 +272,7 @@ class Batch:
             L.tasep_batch_run.argtypes = [H, C.POINTER(_RunCfg), C.c_int, C.POINTER(RunResult), C.POINTER(C.c_int)]
             L.tasep_batch_store.argtypes = [H, C.c_int, _dp]
             L.tasep_batch_densities.argtypes = [H, _dp]
+            L.tasep_batch_last_config.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]
             L._batch_types = True
         self.n, self.nsys = n, nsys
         self._h = H()
@@ -315,6 +317,12 @@ class Batch:
         out = np.empty(1 << self.n)
         _check(lib().tasep_batch_store(self._h, sys, out.ctypes.data_as(_dp)))
         return out
+
+    def last_config(self):
+        """(schedule, states per CTA, CTAs per system) of the last run."""
+        a, b, c = C.c_int(0), C.c_int(0), C.c_int(0)
+        _check(lib().tasep_batch_last_config(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
 
     def densities(self):
         rho = np.empty((self.nsys, self.n))

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "meq_batch.cuh"
+#include "meq_cluster.cuh"
 
 namespace {
 
@@ -75,6 +76,8 @@ struct tasep_batch {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int graph_steps = 0;
     double graph_key[4] = {0, 0, 0, 0};
+    // last run: schedule, states per CTA and CTAs per system
+    int last_schedule = -1, last_states_per_cta = 0, last_ctas_per_system = 0;
 };
 
 namespace {
@@ -131,6 +134,173 @@ tasep_status batch_capture(tasep_batch *b, const BatchParams &base, int sched, i
     e = cudaGraphInstantiate(&b->graph[sched], gr, 0);
     cudaGraphDestroy(gr);
     if (e != cudaSuccess) return fail(TASEP_ERR_CUDA, "graph instantiation: %s", cudaGetErrorString(e));
+    return TASEP_OK;
+}
+
+// ---- cluster-resident engine (schedule 2, n <= kClMaxN) ----
+
+template <typename E> tasep_status cluster_config(int cs_log2, int sbits, cudaLaunchConfig_t &cfg,
+                                                  cudaLaunchAttribute *at, int nclusters, cudaStream_t st) {
+    const size_t smem = ClLayout<E>::bytes(sbits);
+    CU_TRY(cudaFuncSetAttribute(meq_cluster_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    if ((1 << cs_log2) > 8)
+        CU_TRY(cudaFuncSetAttribute(meq_cluster_kernel<E>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3(unsigned(nclusters) << cs_log2);
+    cfg.blockDim = dim3(kClThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 1u << cs_log2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return TASEP_OK;
+}
+
+// Clusters of this shape that can be resident at once (0: the shape does not fit).
+template <typename E> tasep_status cluster_capacity(int cs_log2, int sbits, int *count) {
+    *count = 0;
+    if (ClLayout<E>::bytes(sbits) > size_t(kSmemMax)) return TASEP_OK;
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at[1];
+    tasep_status s = cluster_config<E>(cs_log2, sbits, cfg, at, 1, nullptr);
+    if (s) return s;
+    int num = 0;
+    if (cudaOccupancyMaxActiveClusters(&num, meq_cluster_kernel<E>, &cfg) != cudaSuccess) {
+        cudaGetLastError();  // shape not launchable on this device
+        num = 0;
+    }
+    *count = num;
+    return TASEP_OK;
+}
+
+template <typename E> tasep_status cluster_launch(const ClusterParams &p, int nclusters, cudaStream_t st) {
+    cudaLaunchConfig_t cfg;
+    cudaLaunchAttribute at[1];
+    tasep_status s = cluster_config<E>(p.cs_log2, p.sbits, cfg, at, nclusters, st);
+    if (s) return s;
+    CU_TRY(cudaLaunchKernelEx(&cfg, meq_cluster_kernel<E>, p));
+    return TASEP_OK;
+}
+
+tasep_status cluster_capacity_p(const tasep_batch *b, int cs_log2, int sbits, int *count) {
+    return b->precision == TASEP_PRECISION_MIXED ? cluster_capacity<float>(cs_log2, sbits, count)
+                                                 : cluster_capacity<double>(cs_log2, sbits, count);
+}
+tasep_status cluster_launch_p(const tasep_batch *b, const ClusterParams &p, int nclusters) {
+    return b->precision == TASEP_PRECISION_MIXED ? cluster_launch<float>(p, nclusters, b->stream)
+                                                 : cluster_launch<double>(p, nclusters, b->stream);
+}
+
+bool cluster_eligible(const tasep_batch *b) { return b->n >= kTileBits + 1 && b->n <= kClMaxN; }
+
+// Every system on its own cluster until its exit rule.  With schedule < 0 the
+// autotuner times the feasible shapes - 2^11, 2^12 or 2^13 states per CTA,
+// i.e. 2^(n-11) .. 2^(n-13) CTAs per system - on a short run of copies of
+// the first systems and keeps the fastest.
+tasep_status batch_run_cluster(tasep_batch *b, const tasep_run_config *rc, int schedule, tasep_run_result *res,
+                               int *schedule_used) {
+    const int n = b->n;
+    struct Shape { int cs_log2, sbits, clusters; };
+    std::vector<Shape> shapes;
+    for (int sb = 13; sb >= 11; --sb) {
+        const int cl = n - sb;
+        if (sb > n || cl < 0 || cl > 4) continue;
+        int cap = 0;
+        tasep_status s = cluster_capacity_p(b, cl, sb, &cap);
+        if (s) return s;
+        if (cap > 0) shapes.push_back({cl, sb, cap});
+    }
+    if (shapes.empty()) return fail(TASEP_ERR_UNSUPPORTED, "no cluster shape fits n=%d on this device", n);
+    ClusterParams base;
+    memset(&base, 0, sizeof base);
+    base.n = n;
+    base.nsys = b->nsys;
+    base.h = rc->h;
+    base.rates = b->rates;
+    base.ex = b->ex;
+    base.queue = b->counters;
+    base.error = b->error;
+    base.thresh = rc->stop_tol * rc->h;
+    base.stop_count = rc->stop_count;
+    base.exit_rule = rc->exit_rule;
+    size_t best = 0;
+    if (shapes.size() > 1 && schedule < 0) {
+        // probe: copies of the first systems (the stage buffers are free here), 32 steps each
+        const size_t vec_bytes = (b->precision == TASEP_PRECISION_MIXED ? sizeof(float) : sizeof(double)) * b->N;
+        const int cap = int(std::min<size_t>(size_t(b->nsys), (vec_bytes * b->nsys) / (sizeof(double) * b->N)));
+        cudaEvent_t e0, e1;
+        CU_TRY(cudaEventCreate(&e0));
+        CU_TRY(cudaEventCreate(&e1));
+        float best_ms = 1e30f;
+        for (size_t k = 0; k < shapes.size(); ++k) {
+            const int sys = std::min(cap, std::max(1, shapes[k].clusters));
+            CU_TRY(cudaMemcpyAsync(b->V[0], b->X, sizeof(double) * b->N * sys, cudaMemcpyDeviceToDevice, b->stream));
+            CU_TRY(cudaMemsetAsync(b->counters, 0, sizeof(unsigned), b->stream));
+            CU_TRY(cudaMemsetAsync(b->error, 0, sizeof(int), b->stream));
+            ClusterParams p = base;
+            p.X = static_cast<double *>(b->V[0]);
+            p.cs_log2 = shapes[k].cs_log2;
+            p.sbits = shapes[k].sbits;
+            p.max_steps = 32;
+            p.exit_rule = 0;
+            p.sys_limit = sys;
+            CU_TRY(cudaEventRecord(e0, b->stream));
+            tasep_status s = cluster_launch_p(b, p, std::min(shapes[k].clusters, sys));
+            if (s) return s;
+            CU_TRY(cudaEventRecord(e1, b->stream));
+            CU_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CU_TRY(cudaEventElapsedTime(&ms, e0, e1));
+            // time per system-step with every cluster busy
+            const float per = ms / float(sys) * float(std::min(shapes[k].clusters, sys)) / float(shapes[k].clusters);
+            if (per < best_ms) {
+                best_ms = per;
+                best = k;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        int herr = 0;
+        CU_TRY(cudaMemcpy(&herr, b->error, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) return fail(TASEP_ERR_TIMEOUT, "a bounded device wait expired");
+    }
+    const Shape &sh = shapes[best];
+    ClusterParams p = base;
+    p.X = b->X;
+    p.cs_log2 = sh.cs_log2;
+    p.sbits = sh.sbits;
+    p.max_steps = rc->steps;
+    p.sys_limit = b->nsys;
+    CU_TRY(cudaMemsetAsync(b->ex, 0, sizeof(BatchExit) * b->nsys, b->stream));
+    CU_TRY(cudaMemsetAsync(b->counters, 0, sizeof(unsigned), b->stream));
+    CU_TRY(cudaMemsetAsync(b->error, 0, sizeof(int), b->stream));
+    tasep_status s = cluster_launch_p(b, p, std::min(sh.clusters, b->nsys));
+    if (s) return s;
+    int herr = 0;
+    CU_TRY(cudaMemcpyAsync(&herr, b->error, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    CU_TRY(cudaStreamSynchronize(b->stream));
+    if (herr) return fail(TASEP_ERR_TIMEOUT, "a bounded device wait expired");
+    b->last_schedule = 2;
+    b->last_states_per_cta = 1 << sh.sbits;
+    b->last_ctas_per_system = 1 << sh.cs_log2;
+    if (schedule_used) *schedule_used = 2;
+    if (res) {
+        std::vector<BatchExit> ex(b->nsys);
+        CU_TRY(cudaMemcpy(ex.data(), b->ex, sizeof(BatchExit) * b->nsys, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < b->nsys; ++k) {
+            res[k].steps_done = ex[k].steps_done;
+            res[k].steps_at_stop = ex[k].steps_at_stop;
+            res[k].early_stop = ex[k].early_stop;
+            res[k].converged = ex[k].converged;
+            res[k].last_checksum = ex[k].last_checksum;
+            double t = rc->t0;
+            for (unsigned long long q = 0; q < ex[k].steps_done; ++q) t += rc->h;
+            res[k].t_end = t;
+        }
+    }
     return TASEP_OK;
 }
 
@@ -253,8 +423,11 @@ tasep_status tasep_batch_run(tasep_batch *b, const tasep_run_config *rc, int sch
                              int *schedule_used) {
     if (!b || !rc) return fail(TASEP_ERR_INVALID, "null argument");
     if (!b->rates_set || !b->state_set) return fail(TASEP_ERR_INVALID, "rates or initial state not set");
-    if (schedule < -1 || schedule > 1) return fail(TASEP_ERR_INVALID, "schedule %d", schedule);
+    if (schedule < -1 || schedule > 2) return fail(TASEP_ERR_INVALID, "schedule %d", schedule);
+    if (schedule == 2 && !cluster_eligible(b))
+        return fail(TASEP_ERR_UNSUPPORTED, "the cluster-resident schedule needs %d < n <= %d", kTileBits, kClMaxN);
     CU_TRY(cudaSetDevice(b->device));
+    if (schedule == 2 || (schedule < 0 && cluster_eligible(b))) return batch_run_cluster(b, rc, schedule, res, schedule_used);
     BatchParams base;
     memset(&base, 0, sizeof base);
     base.n = b->n;
@@ -333,6 +506,9 @@ tasep_status tasep_batch_run(tasep_batch *b, const tasep_run_config *rc, int sch
     cudaEventDestroy(e1);
     if (st) return st;
     if (schedule_used) *schedule_used = sched;
+    b->last_schedule = sched;
+    b->last_states_per_cta = kTile;
+    b->last_ctas_per_system = 0;
     if (res) {
         std::vector<BatchExit> ex(b->nsys);
         CU_TRY(cudaMemcpy(ex.data(), b->ex, sizeof(BatchExit) * b->nsys, cudaMemcpyDeviceToHost));
@@ -354,6 +530,15 @@ tasep_status tasep_batch_store(const tasep_batch *b, int sys, double *host_x) {
     if (!b || !host_x || sys < 0 || sys >= b->nsys) return fail(TASEP_ERR_INVALID, "bad argument");
     CU_TRY(cudaSetDevice(b->device));
     CU_TRY(cudaMemcpy(host_x, b->X + size_t(sys) * b->N, sizeof(double) * b->N, cudaMemcpyDeviceToHost));
+    return TASEP_OK;
+}
+
+tasep_status tasep_batch_last_config(const tasep_batch *b, int *schedule, int *states_per_cta,
+                                     int *ctas_per_system) {
+    if (!b) return fail(TASEP_ERR_INVALID, "null handle");
+    if (schedule) *schedule = b->last_schedule;
+    if (states_per_cta) *states_per_cta = b->last_states_per_cta;
+    if (ctas_per_system) *ctas_per_system = b->last_ctas_per_system;
     return TASEP_OK;
 }
 

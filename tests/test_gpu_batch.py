@@ -132,12 +132,66 @@ def test_autotuner_picks_a_valid_schedule_and_changes_no_result():
     n, nsys, steps = 13, 6, 200
     R = sweep_rates(n, nsys, 4)
     out = {}
-    for sched in (-1, 0, 1):
+    for sched in (-1, 0, 1, 2):
         with T.Batch(n, nsys) as b:
             b.set_rates(R)
             b.init(T.INIT_EMPTY)
             res, used = b.run(0.01, steps, exit_rule=False, schedule=sched)
             out[sched] = (used, [b.store(s) for s in range(nsys)])
-    assert out[-1][0] in (0, 1)
+            if sched == -1:
+                cfg = b.last_config()
+    assert out[-1][0] in (0, 1, 2)
+    assert cfg[0] == out[-1][0]
+    if cfg[0] == 2:  # a cluster shape that covers the system: CTAs x states per CTA = 2^n
+        assert cfg[1] in (2048, 4096, 8192) and cfg[1] * cfg[2] == 1 << n
     for s in range(nsys):
         assert np.array_equal(out[-1][1][s], out[out[-1][0]][1][s])
+
+
+
+@pytest.mark.parametrize("n,precision", [(12, T.PRECISION_FP64), (14, T.PRECISION_FP64), (16, T.PRECISION_FP64),
+                                         (17, T.PRECISION_FP64), (15, T.PRECISION_MIXED)])
+def test_cluster_resident_fixed_steps_matches_oracle(n, precision):
+    """Schedule 2 (each system in the shared memory of one cluster, partners in
+    other CTAs read through distributed shared memory), fixed steps: FP64
+    within 1e-12 of the oracle's single-system RK4, mixed densities within 1e-6."""
+    nsys, steps = 5, 150
+    R = sweep_rates(n, nsys, 10 + n)
+    with T.Batch(n, nsys, precision) as b:
+        b.set_rates(R)
+        b.init(T.INIT_EMPTY)
+        res, used = b.run(0.01, steps, exit_rule=False, schedule=2)
+        assert used == 2
+        finals = [b.store(s) for s in range(nsys)]
+        rho = b.densities()
+    for s in range(nsys):
+        xo, _ = O.run(n, R[s], h=0.01, steps=steps, integrator=O.INT_RK4, init=O.INIT_EMPTY, exit_rule=False)
+        assert res[s]["steps_done"] == steps
+        if precision == T.PRECISION_FP64:
+            assert np.max(np.abs(finals[s] - xo)) <= 1e-12
+        else:
+            assert np.max(np.abs(rho[s] - O.densities(n, xo))) <= 1e-6
+            assert abs(finals[s].sum() - 1.0) <= 1e-8
+
+
+def test_cluster_resident_retires_systems_at_their_own_exit():
+    """More systems than clusters, each to its own exit rule: the queue hands
+    out systems as others converge; every one ends where the single-system
+    integrator ends."""
+    n, nsys = 13, 40
+    R = sweep_rates(n, nsys, 21)
+    tol, cap = 1e-7, 200000
+    with T.Batch(n, nsys) as b:
+        b.set_rates(R)
+        b.init(T.INIT_EMPTY)
+        res, used = b.run(0.01, cap, stop_tol=tol, schedule=2)
+        finals = [b.store(s) for s in range(nsys)]
+    assert all(r["converged"] == 1 for r in res)
+    for s in range(0, nsys, 5):
+        with T.Meq(n, T.INTEGRATOR_RK4) as m:
+            m.set_rates(R[s])
+            m.init(T.INIT_EMPTY)
+            rs = m.run(0.01, cap, stop_tol=tol)
+            x = m.store()
+        assert abs(int(rs["steps_done"]) - int(res[s]["steps_done"])) <= 2
+        assert np.max(np.abs(finals[s] - x)) <= 1e-12
