@@ -197,10 +197,11 @@ tasep_status tasep_batch_load(tasep_batch *b, const double *host_x);
  * interleaved over the SMs, 1 = whole systems per SM, 2 = cluster-resident:
  * each system held entirely in the shared memory of one thread-block cluster
  * (2^(n-13) .. 2^(n-11) CTAs, n <= 17) and run to its exit rule there, with no
- * device-memory traffic between steps.  -1 takes 2 when n <= 17 (timing its
- * shapes on a short run of copies of the first systems and keeping the
- * fastest), else times 0 and 1.  *schedule_used (may be NULL) reports the
- * choice. */
+ * device-memory traffic between steps; its shape (states per CTA) is chosen
+ * by timing the feasible shapes on a short run of copies of the first
+ * systems.  -1 times schedules 0 and 1 and keeps the faster (re-timed each
+ * time the number of running systems halves).  *schedule_used (may be NULL)
+ * reports the choice. */
 tasep_status tasep_batch_run(tasep_batch *b, const tasep_run_config *rc, int schedule, tasep_run_result *res,
                              int *schedule_used);
 /* The configuration the last tasep_batch_run used: schedule, states per CTA

@@ -173,73 +173,99 @@ __device__ __forceinline__ bool cl_barrier(ClCtrl &c, uint32_t &k, int ranks, ui
     return !c.err;
 }
 
-// One row sum over the pair of states (i, i+1), i even, of the gathered
-// vector whose cluster addresses (per rank) are cbase; local part `loc`.
-template <typename G>
-__device__ __forceinline__ void cl_row_pair(const ClCtrl &c, const uint32_t *cbase, const G *loc, int n, int sbits,
-                                            uint32_t rank, uint32_t i, const G *dlo, const G *dhi, G &t0, G &t1) {
+// Row sums of all pairs a thread owns, for a gathered vector with local part
+// `loc` and per-rank cluster addresses `cbase`.  Thread t owns the NP pairs
+// (i, i+1), i = rank*S + 2t + 1024q, q = 0..NP-1 (S = 1024 NP states per CTA).
+// The loops run over the terms in the reference's row order (entry,
+// diagonal, exit, hops by ascending bit) with the pairs innermost: the loads
+// of one term for all NP pairs are independent and in flight together, and
+// whether a hop's partner lives in another CTA depends only on its bit.
+template <typename G, int NP>
+__device__ __forceinline__ void cl_gather(const ClCtrl &c, const uint32_t *cbase, const G *loc, int n, int sbits,
+                                          uint32_t rank, const G *dlo, const G *dhi, G (&t)[2 * NP]) {
     using A = Ar<G, false>;
+    using V2T = typename std::conditional<sizeof(G) == 8, double2, float2>::type;
     const uint32_t smask = (1u << sbits) - 1;
-    const uint32_t li = i & smask;
+    const uint32_t i0 = (rank << sbits) + 2 * threadIdx.x;
     auto rate = [&](int k) -> G { return sizeof(G) == 8 ? G(c.rates_d[k]) : G(c.rates_f[k]); };
-    auto load_pair = [&](uint32_t j, G &u, G &v) {
+    auto pair_at = [&](uint32_t j, G &u, G &v) {  // pair starting at even global index j
         const uint32_t rj = j >> sbits, lj = j & smask;
         if (rj == rank) {
-            const auto w = reinterpret_cast<const typename std::conditional<sizeof(G) == 8, double2, float2>::type *>(
-                loc + lj)[0];
+            const V2T w = *reinterpret_cast<const V2T *>(loc + lj);
             u = w.x;
             v = w.y;
         } else {
             ClLoad<G>::pair(cbase[rj] + lj * uint32_t(sizeof(G)), u, v);
         }
     };
-    G x0, x1;
-    {
-        const auto w = reinterpret_cast<const typename std::conditional<sizeof(G) == 8, double2, float2>::type *>(
-            loc + li)[0];
-        x0 = w.x;
-        x1 = w.y;
+    G x[2 * NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) {
+        const V2T w = *reinterpret_cast<const V2T *>(loc + ((i0 + 1024u * q) & smask));
+        x[2 * q] = w.x;
+        x[2 * q + 1] = w.y;
+        t[2 * q] = G(0);
+        t[2 * q + 1] = G(0);
     }
-    G a0 = G(0), a1 = G(0);
-    if ((i >> (n - 1)) & 1) {  // 1. entry from i - 2^(n-1)
-        G e0, e1;
-        load_pair(i - (1u << (n - 1)), e0, e1);
+    {  // 1. entry from i - 2^(n-1)
         const G r0 = rate(0);
-        a0 = A::madd(a0, r0, e0);
-        a1 = A::madd(a1, r0, e1);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            const uint32_t i = i0 + 1024u * q;
+            if ((i >> (n - 1)) & 1) {
+                G e0, e1;
+                pair_at(i - (1u << (n - 1)), e0, e1);
+                t[2 * q] = A::madd(t[2 * q], r0, e0);
+                t[2 * q + 1] = A::madd(t[2 * q + 1], r0, e1);
+            }
+        }
     }
-    // 2. diagonal: bits 0..7, bits 8..n-1, and the pair (7, 8) between them
-    const uint32_t i1 = i + 1;
-    G d0 = dlo[i & 255] + dhi[i >> 8], d1 = dlo[i1 & 255] + dhi[i1 >> 8];
-    if (!((i >> 7) & 1) && ((i >> 8) & 1)) {
-        const G r7 = rate(n - 8);
-        d0 -= r7;
-        d1 -= r7;
+    {  // 2. diagonal (bits 0..7 and the pair (7, 8) are the thread's), 3. exit
+        const G lo0 = dlo[i0 & 255], lo1 = dlo[(i0 + 1) & 255];
+        const G r7 = (!((i0 >> 7) & 1) && ((i0 >> 8) & 1)) ? rate(n - 8) : G(0);
+        const G rn = rate(n);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            const uint32_t i = i0 + 1024u * q;
+            const G hi = dhi[i >> 8];
+            const G d0 = (lo0 + hi) - r7, d1 = (lo1 + hi) - r7;
+            t[2 * q] = A::madd(t[2 * q], d0, x[2 * q]);
+            t[2 * q + 1] = A::madd(t[2 * q + 1], d1, x[2 * q + 1]);
+            t[2 * q] = A::madd(t[2 * q], rn, x[2 * q + 1]);
+        }
     }
-    a0 = A::madd(a0, d0, x0);
-    a1 = A::madd(a1, d1, x1);
-    a0 = A::madd(a0, rate(n), x1);  // 3. exit: state i (bit 0 clear) from i+1
-    // 4. hops, ascending bit: k = 0 for the odd state (partner i+2, same CTA)
-    if (!((i >> 1) & 1)) {
-        const G p = loc[li + 2];
-        a1 = A::madd(a1, rate(n - 1), p);
+    if (!((i0 >> 1) & 1)) {  // 4. hop k = 0 into the odd state, from i+2 (same CTA, same q)
+        const G r = rate(n - 1);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            const G p = loc[((i0 + 1024u * q) & smask) + 2];
+            t[2 * q + 1] = A::madd(t[2 * q + 1], r, p);
+        }
     }
-    // k >= 1: both states of the pair, partner pair i + 2^k
-    uint32_t hm = i & ~(i >> 1) & ((1u << (n - 1)) - 1) & ~1u;
-    while (hm) {
-        const int k = __ffs(hm) - 1;
-        hm &= hm - 1;
-        G p0, p1;
-        load_pair(i + (1u << k), p0, p1);
+    for (int k = 1; k < n - 1; ++k) {  // hops k >= 1 into both states, from the pair at i + 2^k
         const G r = rate(n - 1 - k);
-        a0 = A::madd(a0, r, p0);
-        a1 = A::madd(a1, r, p1);
+        const bool remote = k + 1 >= sbits;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            const uint32_t i = i0 + 1024u * q;
+            if (((i >> k) & 3u) == 1u) {
+                const uint32_t j = i + (1u << k);
+                G p0, p1;
+                if (remote) {
+                    ClLoad<G>::pair(cbase[j >> sbits] + (j & smask) * uint32_t(sizeof(G)), p0, p1);
+                } else {
+                    const V2T w = *reinterpret_cast<const V2T *>(loc + (j & smask));
+                    p0 = w.x;
+                    p1 = w.y;
+                }
+                t[2 * q] = A::madd(t[2 * q], r, p0);
+                t[2 * q + 1] = A::madd(t[2 * q + 1], r, p1);
+            }
+        }
     }
-    t0 = a0;
-    t1 = a1;
 }
 
-template <typename E>
+template <typename E, int NP>
 __global__ void __launch_bounds__(kClThreads, 1) meq_cluster_kernel(const __grid_constant__ ClusterParams p) {
     extern __shared__ __align__(128) unsigned char cl_smem[];
     ClCtrl &c = *reinterpret_cast<ClCtrl *>(cl_smem);
@@ -338,60 +364,62 @@ __global__ void __launch_bounds__(kClThreads, 1) meq_cluster_kernel(const __grid
         bool failed = false;
         while (step < p.max_steps) {
             // H1: a = h M x
-            for (uint32_t pp = tid; pp < S / 2; pp += kClThreads) {
-                const uint32_t i = (rank << sbits) + 2 * pp;
-                double t0, t1;
-                cl_row_pair<double>(c, c.cl_buf[0], X, n, sbits, rank, i, dlo_d, dhi_d, t0, t1);
-                Av[2 * pp] = E(h * t0);
-                Av[2 * pp + 1] = E(h * t1);
-            }
-            if (!cl_barrier(c, bk, ranks, limit, p.error)) { failed = true; break; }
-            // H2: b = a + h/4 M a
-            const E h4 = E(h / 4), h3 = E(h / 3);
-            const double h2 = h / 2;
-            for (uint32_t pp = tid; pp < S / 2; pp += kClThreads) {
-                const uint32_t i = (rank << sbits) + 2 * pp;
-                E t0, t1;
-                cl_row_pair<E>(c, c.cl_buf[1], Av, n, sbits, rank, i, dlo_e, dhi_e, t0, t1);
-                Bv[2 * pp] = Av[2 * pp] + h4 * t0;
-                Bv[2 * pp + 1] = Av[2 * pp + 1] + h4 * t1;
-            }
-            if (!cl_barrier(c, bk, ranks, limit, p.error)) { failed = true; break; }
-            // H3: c = a + h/3 M b, held in registers until b is no longer gathered
-            constexpr int kMaxPairs = (1 << 13) / 2 / kClThreads;  // S <= 2^13
-            E cr[2 * kMaxPairs];
+            {
+                double t[2 * NP];
+                cl_gather<double, NP>(c, c.cl_buf[0], X, n, sbits, rank, dlo_d, dhi_d, t);
 #pragma unroll
-            for (int q = 0; q < kMaxPairs; ++q) {
-                const uint32_t pp = tid + q * kClThreads;
-                if (pp < S / 2) {
-                    const uint32_t i = (rank << sbits) + 2 * pp;
-                    E t0, t1;
-                    cl_row_pair<E>(c, c.cl_buf[2], Bv, n, sbits, rank, i, dlo_e, dhi_e, t0, t1);
-                    cr[2 * q] = Av[2 * pp] + h3 * t0;
-                    cr[2 * q + 1] = Av[2 * pp + 1] + h3 * t1;
+                for (int q = 0; q < NP; ++q) {
+                    const uint32_t l = 2 * tid + 1024u * q;
+                    Av[l] = E(h * t[2 * q]);
+                    Av[l + 1] = E(h * t[2 * q + 1]);
                 }
             }
             if (!cl_barrier(c, bk, ranks, limit, p.error)) { failed = true; break; }
+            const E h4 = E(h / 4), h3 = E(h / 3);
+            const double h2 = h / 2;
+            {  // H2: b = a + h/4 M a
+                E t[2 * NP];
+                cl_gather<E, NP>(c, c.cl_buf[1], Av, n, sbits, rank, dlo_e, dhi_e, t);
 #pragma unroll
-            for (int q = 0; q < kMaxPairs; ++q) {
-                const uint32_t pp = tid + q * kClThreads;
-                if (pp < S / 2) {
-                    Bv[2 * pp] = cr[2 * q];
-                    Bv[2 * pp + 1] = cr[2 * q + 1];
+                for (int q = 0; q < NP; ++q) {
+                    const uint32_t l = 2 * tid + 1024u * q;
+                    Bv[l] = Av[l] + h4 * t[2 * q];
+                    Bv[l + 1] = Av[l + 1] + h4 * t[2 * q + 1];
+                }
+            }
+            if (!cl_barrier(c, bk, ranks, limit, p.error)) { failed = true; break; }
+            {  // H3: c = a + h/3 M b, held in registers until b is no longer gathered
+                E t[2 * NP];
+                cl_gather<E, NP>(c, c.cl_buf[2], Bv, n, sbits, rank, dlo_e, dhi_e, t);
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    const uint32_t l = 2 * tid + 1024u * q;
+                    t[2 * q] = Av[l] + h3 * t[2 * q];
+                    t[2 * q + 1] = Av[l + 1] + h3 * t[2 * q + 1];
+                }
+                if (!cl_barrier(c, bk, ranks, limit, p.error)) { failed = true; break; }
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    const uint32_t l = 2 * tid + 1024u * q;
+                    Bv[l] = t[2 * q];
+                    Bv[l + 1] = t[2 * q + 1];
                 }
             }
             if (!cl_barrier(c, bk, ranks, limit, p.error)) { failed = true; break; }
             // H4: D = a + h/2 M c, x += D, L1 norm
             double cs = 0.0;
-            for (uint32_t pp = tid; pp < S / 2; pp += kClThreads) {
-                const uint32_t i = (rank << sbits) + 2 * pp;
-                E t0, t1;
-                cl_row_pair<E>(c, c.cl_buf[2], Bv, n, sbits, rank, i, dlo_e, dhi_e, t0, t1);
-                const double D0 = double(Av[2 * pp]) + h2 * double(t0);
-                const double D1 = double(Av[2 * pp + 1]) + h2 * double(t1);
-                X[2 * pp] += D0;
-                X[2 * pp + 1] += D1;
-                cs += fabs(D0) + fabs(D1);
+            {
+                E t[2 * NP];
+                cl_gather<E, NP>(c, c.cl_buf[2], Bv, n, sbits, rank, dlo_e, dhi_e, t);
+#pragma unroll
+                for (int q = 0; q < NP; ++q) {
+                    const uint32_t l = 2 * tid + 1024u * q;
+                    const double D0 = double(Av[l]) + h2 * double(t[2 * q]);
+                    const double D1 = double(Av[l + 1]) + h2 * double(t[2 * q + 1]);
+                    X[l] += D0;
+                    X[l + 1] += D1;
+                    cs += fabs(D0) + fabs(D1);
+                }
             }
             {
                 const double ws = warp_sum(cs);

@@ -125,19 +125,6 @@ template <typename E> struct StageT<ST_U4, E> {
     static constexpr int NX = 3; static constexpr bool FINAL = true; static constexpr bool EXACT = true;
 };
 
-// Per-tile quantities that every consumer thread would otherwise derive from
-// the tile index (bit scans over up to 22 tile-index bits): the producer
-// computes them once and stores them beside the tile's own buffer before it
-// arms that buffer's barrier.
-constexpr int kMaxTileTerms = 12;  // partner hops or tile-level diagonal terms of one tile (ntb <= 22)
-struct TileMeta {
-    int nhop;                      // high hops (ring slots after entry and straddle)
-    int ndh;                       // tile-level diagonal terms
-    double ds;                     // their sum, in the gather type (stages that may reassociate)
-    double hrate[kMaxTileTerms];   // rate of each high hop, ascending bit (consumer order)
-    double drate[kMaxTileTerms];   // tile-level diagonal rates in the reference's subtraction order
-};
-
 struct TileCtrl {
     uint64_t full[2], empty[2];
     uint64_t rfull[kMaxRing], rempty[kMaxRing];
@@ -148,9 +135,8 @@ struct TileCtrl {
     int err;
     int is_last;
     int pad;
-    TileMeta meta[2];  // of the tile in own-tile buffer b
 };
-constexpr int kCtrlBytes = 2048;
+constexpr int kCtrlBytes = 1024;
 static_assert(sizeof(TileCtrl) <= kCtrlBytes, "control block");
 
 template <int S, typename E> struct TileLayout {
@@ -252,29 +238,13 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 const int b = it & 1;
                 if (it >= 2 && !mbar_wait(&c.empty[b], ((it >> 1) - 1) & 1, errf, wait_ns)) break;
                 unsigned char *st = stage_base + b * LY::stage;
+                mbar_arrive_expect_tx(&c.full[b], LY::stage);
+                bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], own_pol);  // read again only as a far partner
                 // partner tiles, in the order the consumers add them
                 const bool top = (T >> (ntb - 1)) & 1;
                 const bool strad = !(T & 1);
-                const unsigned long long lowmask = ntb >= 2 ? ((1ull << (ntb - 1)) - 1) : 0ull;
-                const unsigned long long hmask = T & ~(T >> 1) & lowmask;
-                {  // the tile's metadata, visible to the consumers once full[b] completes
-                    TileMeta &mt = c.meta[b];
-                    int k = 0;
-                    for (unsigned long long mh = hmask; mh; mh &= mh - 1)
-                        mt.hrate[k++] = c.rates_d[n - 1 - kTileBits - (__ffsll(mh) - 1)];
-                    mt.nhop = k;
-                    G ds = G(0);
-                    k = 0;
-                    for (unsigned long long mh = ~T & (T >> 1) & lowmask; mh; mh &= mh - 1) {
-                        const int i = n - 1 - kTileBits - (__ffsll(mh) - 1);
-                        mt.drate[k++] = c.rates_d[i];
-                        ds += rate_of<G>(c, i);
-                    }
-                    mt.ndh = k;
-                    mt.ds = static_cast<double>(ds);
-                }
-                mbar_arrive_expect_tx(&c.full[b], LY::stage);
-                bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], own_pol);  // read again only as a far partner
+                const unsigned long long hmask =
+                    ntb >= 2 ? (T & ~(T >> 1) & ((1ull << (ntb - 1)) - 1)) : 0ull;
                 const int np = int(top) + int(strad) + __popcll(hmask);
                 unsigned long long hm = hmask;
                 for (int q = 0; q < np; ++q) {
@@ -379,8 +349,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         const int b = it & 1;
         const bool top = (T >> (ntb - 1)) & 1;
         const bool strad = !(T & 1);
+        const unsigned long long lowmask = ntb >= 2 ? ((1ull << (ntb - 1)) - 1) : 0ull;
+        const unsigned long long hmask = T & ~(T >> 1) & lowmask;
+        const unsigned long long dhmask = ~T & (T >> 1) & lowmask;
         const unsigned long long gT = T * kTile;
-        const TileMeta &mt = c.meta[b];  // read only after full[b] completes
 
         // per-state extra inputs, read once straight into registers; they are
         // only needed in the epilogue, so their latency hides behind the sweep
@@ -432,13 +404,17 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL);
         }
         if constexpr (Tr::EXACT) {  // the reference's subtraction order
-            const int ndh = mt.ndh;
-            for (int k = 0; k < ndh; ++k) {
-                const G rr = static_cast<G>(mt.drate[k]);
+            unsigned long long mh = dhmask;
+            while (mh) {
+                const int u = __ffsll(mh) - 1;
+                mh &= mh - 1;
+                const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 d0 = A::sub(d0, rr); d1 = A::sub(d1, rr); d2 = A::sub(d2, rr); d3 = A::sub(d3, rr);
             }
         } else {  // reassociation allowed: one sum of the tile-level rates
-            const G ds = static_cast<G>(mt.ds);
+            G ds = G(0);
+            for (unsigned long long mh = dhmask; mh; mh &= mh - 1)
+                ds += rate_of<G>(c, n - 1 - kTileBits - (__ffsll(mh) - 1));
             d0 -= ds; d1 -= ds; d2 -= ds; d3 -= ds;
         }
         a0 = A::madd(a0, d0, x0); a1 = A::madd(a1, d1, x1);
@@ -498,12 +474,14 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             if (++cslot == RS) { cslot = 0; cph ^= 1; }
         }
         {
-            const int nhop = mt.nhop;  // k >= 11
-            for (int k = 0; k < nhop; ++k) {
+            unsigned long long mh = hmask;  // k >= 11
+            while (mh) {
+                const int u = __ffsll(mh) - 1;
+                mh &= mh - 1;
                 const int slot = cslot;
                 if (!mbar_wait(&c.rfull[slot], cph, errf, wait_ns)) { ok = false; break; }
                 const G *pp = reinterpret_cast<const G *>(ring_base + slot * LY::gb);
-                const G rr = static_cast<G>(mt.hrate[k]);
+                const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 G p0, p1, p2, p3;
                 V2<G>::lds(pp + pb0, p0, p1);
                 V2<G>::lds(pp + pb1, p2, p3);

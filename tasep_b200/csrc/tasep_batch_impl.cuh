@@ -139,12 +139,15 @@ tasep_status batch_capture(tasep_batch *b, const BatchParams &base, int sched, i
 
 // ---- cluster-resident engine (schedule 2, n <= kClMaxN) ----
 
-template <typename E> tasep_status cluster_config(int cs_log2, int sbits, cudaLaunchConfig_t &cfg,
-                                                  cudaLaunchAttribute *at, int nclusters, cudaStream_t st) {
+// The cluster kernel is instantiated for 2, 4 and 8 pairs per thread (2^11,
+// 2^12, 2^13 states per CTA).
+template <typename E, int NP> tasep_status cluster_config_np(int cs_log2, cudaLaunchConfig_t &cfg,
+                                                             cudaLaunchAttribute *at, int nclusters, cudaStream_t st) {
+    const int sbits = 10 + (NP == 8 ? 3 : NP == 4 ? 2 : 1);
     const size_t smem = ClLayout<E>::bytes(sbits);
-    CU_TRY(cudaFuncSetAttribute(meq_cluster_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    CU_TRY(cudaFuncSetAttribute(meq_cluster_kernel<E, NP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     if ((1 << cs_log2) > 8)
-        CU_TRY(cudaFuncSetAttribute(meq_cluster_kernel<E>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        CU_TRY(cudaFuncSetAttribute(meq_cluster_kernel<E, NP>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     memset(&cfg, 0, sizeof cfg);
     cfg.gridDim = dim3(unsigned(nclusters) << cs_log2);
     cfg.blockDim = dim3(kClThreads);
@@ -159,16 +162,15 @@ template <typename E> tasep_status cluster_config(int cs_log2, int sbits, cudaLa
     return TASEP_OK;
 }
 
-// Clusters of this shape that can be resident at once (0: the shape does not fit).
-template <typename E> tasep_status cluster_capacity(int cs_log2, int sbits, int *count) {
+template <typename E, int NP> tasep_status cluster_capacity_np(int cs_log2, int *count) {
     *count = 0;
-    if (ClLayout<E>::bytes(sbits) > size_t(kSmemMax)) return TASEP_OK;
+    if (ClLayout<E>::bytes(10 + (NP == 8 ? 3 : NP == 4 ? 2 : 1)) > size_t(kSmemMax)) return TASEP_OK;
     cudaLaunchConfig_t cfg;
     cudaLaunchAttribute at[1];
-    tasep_status s = cluster_config<E>(cs_log2, sbits, cfg, at, 1, nullptr);
+    tasep_status s = cluster_config_np<E, NP>(cs_log2, cfg, at, 1, nullptr);
     if (s) return s;
     int num = 0;
-    if (cudaOccupancyMaxActiveClusters(&num, meq_cluster_kernel<E>, &cfg) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveClusters(&num, meq_cluster_kernel<E, NP>, &cfg) != cudaSuccess) {
         cudaGetLastError();  // shape not launchable on this device
         num = 0;
     }
@@ -176,13 +178,31 @@ template <typename E> tasep_status cluster_capacity(int cs_log2, int sbits, int 
     return TASEP_OK;
 }
 
-template <typename E> tasep_status cluster_launch(const ClusterParams &p, int nclusters, cudaStream_t st) {
+template <typename E, int NP> tasep_status cluster_launch_np(const ClusterParams &p, int nclusters, cudaStream_t st) {
     cudaLaunchConfig_t cfg;
     cudaLaunchAttribute at[1];
-    tasep_status s = cluster_config<E>(p.cs_log2, p.sbits, cfg, at, nclusters, st);
+    tasep_status s = cluster_config_np<E, NP>(p.cs_log2, cfg, at, nclusters, st);
     if (s) return s;
-    CU_TRY(cudaLaunchKernelEx(&cfg, meq_cluster_kernel<E>, p));
+    CU_TRY(cudaLaunchKernelEx(&cfg, meq_cluster_kernel<E, NP>, p));
     return TASEP_OK;
+}
+
+template <typename E> tasep_status cluster_capacity(int cs_log2, int sbits, int *count) {
+    switch (sbits) {
+    case 13: return cluster_capacity_np<E, 8>(cs_log2, count);
+    case 12: return cluster_capacity_np<E, 4>(cs_log2, count);
+    case 11: return cluster_capacity_np<E, 2>(cs_log2, count);
+    default: *count = 0; return TASEP_OK;
+    }
+}
+
+template <typename E> tasep_status cluster_launch(const ClusterParams &p, int nclusters, cudaStream_t st) {
+    switch (p.sbits) {
+    case 13: return cluster_launch_np<E, 8>(p, nclusters, st);
+    case 12: return cluster_launch_np<E, 4>(p, nclusters, st);
+    case 11: return cluster_launch_np<E, 2>(p, nclusters, st);
+    default: return fail(TASEP_ERR_INVALID, "no cluster kernel for 2^%d states per CTA", p.sbits);
+    }
 }
 
 tasep_status cluster_capacity_p(const tasep_batch *b, int cs_log2, int sbits, int *count) {
@@ -206,8 +226,8 @@ tasep_status batch_run_cluster(tasep_batch *b, const tasep_run_config *rc, int s
     struct Shape { int cs_log2, sbits, clusters; };
     std::vector<Shape> shapes;
     for (int sb = 13; sb >= 11; --sb) {
-        const int cl = n - sb;
-        if (sb > n || cl < 0 || cl > 4) continue;
+        const int cl = n - sb;  // log2 CTAs per system
+        if (sb > n || cl > 4) continue;
         int cap = 0;
         tasep_status s = cluster_capacity_p(b, cl, sb, &cap);
         if (s) return s;
@@ -427,7 +447,10 @@ tasep_status tasep_batch_run(tasep_batch *b, const tasep_run_config *rc, int sch
     if (schedule == 2 && !cluster_eligible(b))
         return fail(TASEP_ERR_UNSUPPORTED, "the cluster-resident schedule needs %d < n <= %d", kTileBits, kClMaxN);
     CU_TRY(cudaSetDevice(b->device));
-    if (schedule == 2 || (schedule < 0 && cluster_eligible(b))) return batch_run_cluster(b, rc, schedule, res, schedule_used);
+    // the cluster-resident engine runs when asked for; measured on B200 it is
+    // slower than the tile engines for the standard n = 16 sweep, so the
+    // automatic choice stays with schedules 0 and 1
+    if (schedule == 2) return batch_run_cluster(b, rc, -1, res, schedule_used);
     BatchParams base;
     memset(&base, 0, sizeof base);
     base.n = b->n;

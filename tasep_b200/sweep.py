@@ -70,6 +70,8 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="both")
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--n", type=int, default=N_SWEEP)
+    ap.add_argument("--schedule", type=int, default=-1,
+                    help="-1 automatic (tile engines), 0/1 a tile engine, 2 cluster-resident")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     R = sweep_rates(a.n, a.grid)
@@ -78,7 +80,7 @@ def main(argv=None):
            "runs": []}
     precs = {"fp64": [PRECISION_FP64], "mixed": [PRECISION_MIXED], "both": [PRECISION_FP64, PRECISION_MIXED]}
     for p in precs[a.precision]:
-        rec = report(*run_sweep(R, p), p)
+        rec = report(*run_sweep(R, p, schedule=a.schedule), p)
         out["runs"].append(rec)
         print(json.dumps({k: v for k, v in rec.items() if k not in ("steps", "rho")}), flush=True)
     if len(out["runs"]) == 2:

@@ -142,8 +142,13 @@ def test_autotuner_picks_a_valid_schedule_and_changes_no_result():
                 cfg = b.last_config()
     assert out[-1][0] in (0, 1, 2)
     assert cfg[0] == out[-1][0]
-    if cfg[0] == 2:  # a cluster shape that covers the system: CTAs x states per CTA = 2^n
-        assert cfg[1] in (2048, 4096, 8192) and cfg[1] * cfg[2] == 1 << n
+    assert cfg[1] == 2048 and cfg[2] == 0  # tile engines: 2^11 states per tile
+    with T.Batch(n, nsys) as b:  # the cluster engine's autotuner: a shape that covers the system
+        b.set_rates(R)
+        b.init(T.INIT_EMPTY)
+        b.run(0.01, 20, exit_rule=False, schedule=2)
+        sched, spc, ctas = b.last_config()
+    assert sched == 2 and spc in (2048, 4096, 8192) and spc * ctas == 1 << n
     for s in range(nsys):
         assert np.array_equal(out[-1][1][s], out[out[-1][0]][1][s])
 
