@@ -172,7 +172,11 @@ template <typename G> __device__ __forceinline__ G rate_of(const TileCtrl &c, in
 template <> __device__ __forceinline__ double rate_of<double>(const TileCtrl &c, int i) { return c.rates_d[i]; }
 template <> __device__ __forceinline__ float rate_of<float>(const TileCtrl &c, int i) { return c.rates_f[i]; }
 
-template <int S, typename E>
+// kTuned: the instantiation that honours a non-default L2 policy and the
+// wait-expiry test hook.  The default launch uses the lean one: the producer
+// thread that issues the bulk copies is on the sweep's critical path, and the
+// per-copy policy selection alone cost 2-3 % of the step time.
+template <int S, typename E, bool kTuned>
 __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_constant__ TileParams p) {
     using Tr = StageT<S, E>;
     using G = typename Tr::G;
@@ -226,11 +230,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             const uint64_t keep = policy_evict_last();    // near partners: read again as own tile soon
             const uint64_t normal = policy_evict_normal();
             const uint64_t first = policy_evict_first();
-            const uint64_t own_pol = (p.l2_flags & L2F_OWN_FIRST) ? first : normal;
-            const uint64_t far_pol = (p.l2_flags & L2F_FAR_FIRST) ? first : keep;
-            const uint64_t ent_pol = (p.l2_flags & L2F_DEMOTE) ? normal : keep;
+            const uint64_t own_pol = (kTuned && (p.l2_flags & L2F_OWN_FIRST)) ? first : normal;
+            const uint64_t far_pol = (kTuned && (p.l2_flags & L2F_FAR_FIRST)) ? first : keep;
+            const uint64_t ent_pol = (kTuned && (p.l2_flags & L2F_DEMOTE)) ? normal : keep;
             const int near = p.l2_near;
-            const bool skip_copy = p.skip_copy_plus1 > 0 && blockIdx.x == 0;
+            const bool skip_copy = kTuned && p.skip_copy_plus1 > 0 && blockIdx.x == 0;
             uint32_t it = 0, cur = 0;
             bool ok = true;
             for (unsigned long long ord = blockIdx.x; ord < p.ntiles && ok; ord += gridDim.x, ++it) {
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                     uint64_t pol = keep;
                     if (q == 0 && top) {
                         src = T - (1ull << (ntb - 1));
-                        pol = ent_pol;
+                        if constexpr (kTuned) pol = ent_pol;
                     } else if (q == int(top) && strad) {
                         src = T + 1;
                         bytes = LY::gb / 2;
@@ -261,14 +265,15 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                         const int u = __ffsll(hm) - 1;
                         hm &= hm - 1;
                         src = T + (1ull << u);
-                        if (u >= near) pol = far_pol;
+                        if constexpr (kTuned)
+                            if (u >= near) pol = far_pol;
                     }
                     const int slot = cur % RS;
                     if (cur >= RS && !mbar_wait(&c.rempty[slot], ((cur / RS) - 1) & 1, errf, wait_ns)) {
                         ok = false;
                         break;
                     }
-                    if (!(skip_copy && cur + 1 == uint32_t(p.skip_copy_plus1))) {
+                    if (!(kTuned && skip_copy && cur + 1 == uint32_t(p.skip_copy_plus1))) {
                         mbar_arrive_expect_tx(&c.rfull[slot], bytes);
                         bulk_g2s(ring_base + slot * LY::gb, g + src * kTile, bytes, &c.rfull[slot], pol);
                     }
@@ -314,7 +319,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     consumer_sync();
 
     const uint64_t once = policy_evict_first();
-    const bool demote = (p.l2_flags & L2F_DEMOTE) != 0;
+    const bool demote = kTuned && (p.l2_flags & L2F_DEMOTE) != 0;
     O *__restrict__ out = static_cast<O *>(p.out);
     const uint32_t t9 = tid;              // state bits 1..9
     const int pb0 = 2 * tid;              // local index of P0

@@ -73,19 +73,25 @@ tasep_status get_scratch(int dev, DevScratch **out) {
     return TASEP_OK;
 }
 
-template <int S, typename E> tasep_status launch_tile(const TileParams &p, int grid, cudaStream_t st) {
+template <int S, typename E, bool kTuned> tasep_status launch_tile_t(const TileParams &p, int grid, cudaStream_t st) {
     // set once per device; concurrent first calls may both set it (idempotent)
     static std::atomic<bool> configured[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     const int bytes = TileLayout<S, E>::bytes;
     if (!configured[dev & 63].load(std::memory_order_acquire)) {
-        CU_TRY(cudaFuncSetAttribute(meq_tile_kernel<S, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        CU_TRY(cudaFuncSetAttribute(meq_tile_kernel<S, E, kTuned>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         configured[dev & 63].store(true, std::memory_order_release);
     }
-    meq_tile_kernel<S, E><<<grid, kTileThreads, bytes, st>>>(p);
+    meq_tile_kernel<S, E, kTuned><<<grid, kTileThreads, bytes, st>>>(p);
     CU_TRY(cudaGetLastError());
     return TASEP_OK;
+}
+
+// The lean instantiation unless a non-default L2 policy or the test hook is set.
+template <int S, typename E> tasep_status launch_tile(const TileParams &p, int grid, cudaStream_t st) {
+    if (p.l2_near < 64 || p.l2_flags || p.skip_copy_plus1) return launch_tile_t<S, E, true>(p, grid, st);
+    return launch_tile_t<S, E, false>(p, grid, st);
 }
 
 template <typename E> tasep_status launch_small(const SmallParams &p, cudaStream_t st) {
