@@ -8,10 +8,12 @@ system ~ U[0.5, 1.5] from numpy's default_rng(2); h = 0.01, empty lattice,
 each system classical RK4 to its own exit rule (|dP| < 1e-10 h on more than
 100 consecutive steps, src/masterEquation.c:670-679).
 
-    python -m tasep_b200.sweep [--precision fp64|mixed|both] [--out report.json]
+    python -m tasep_b200.sweep [--precision fp64|mixed|both] [--schedule S] [--out report.json]
+    python -m tasep_b200.sweep --cost-profile [--schedule S]
 
 writes per-system exit steps and final densities, the sweep's wall time and
-the schedule the autotuner chose.
+the schedule the autotuner chose; --cost-profile prints the time of one step
+against the number of systems running.
 """
 from __future__ import annotations
 
@@ -51,6 +53,27 @@ def run_sweep(rates, precision=PRECISION_FP64, h=0.01, max_steps=2_000_000, stop
     return res, rho, sec, used
 
 
+def cost_profile(n=N_SWEEP, counts=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024), steps=512, schedule=-1,
+                 precision=PRECISION_FP64):
+    """Device time per step of the batched integrator against the number of
+    systems running (the standard sweep's first systems, no exit rule): the
+    cost a sweep pays at each point of its retirement curve."""
+    R = sweep_rates(n)
+    out = []
+    for k in counts:
+        with Batch(n, k, precision) as b:
+            b.set_rates(R[:k])
+            b.init(INIT_EMPTY)
+            b.run(0.01, 32, exit_rule=False, schedule=schedule)  # warm-up (and the autotuner's probes)
+            t0 = time.perf_counter()
+            b.run(0.01, steps, exit_rule=False, schedule=schedule)
+            sec = time.perf_counter() - t0
+            sched, spc, ctas = b.last_config()
+        out.append({"systems": k, "us_per_step": sec / steps * 1e6, "schedule": sched, "states_per_cta": spc,
+                    "ctas_per_system": ctas})
+    return out
+
+
 def report(res, rho, sec, used, precision):
     steps = np.array([r["steps_done"] for r in res], dtype=np.int64)
     n = rho.shape[1]
@@ -72,8 +95,14 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=N_SWEEP)
     ap.add_argument("--schedule", type=int, default=-1,
                     help="-1 automatic (tile engines), 0/1 a tile engine, 2 cluster-resident")
+    ap.add_argument("--cost-profile", action="store_true",
+                    help="only time one step against the number of running systems")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
+    if a.cost_profile:
+        for rec in cost_profile(a.n, schedule=a.schedule):
+            print(json.dumps(rec), flush=True)
+        return
     R = sweep_rates(a.n, a.grid)
     out = {"workload": f"{a.grid * a.grid} systems, n={a.n}, (alpha, beta) on a {a.grid}x{a.grid} grid over "
                        f"[0.05, 1.5]^2, hops U[0.5, 1.5] seed 2, h=0.01, empty start, exit 1e-10*h / 100 steps",
