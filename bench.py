@@ -48,8 +48,10 @@ ALG_BYTES = {
     ("meq_ref_step", 0): 16, ("meq_rk4_h1", 0): 16, ("meq_rk4_h2", 0): 16, ("meq_rk4_h3", 0): 24,
     ("meq_rk4_h4", 0): 32, ("meq_rk4_h1", 1): 12, ("meq_rk4_h2", 1): 8, ("meq_rk4_h3", 1): 12,
     ("meq_rk4_h4", 1): 24,
+    # time-variant RK4: materialised stage inputs (u2, u3, u4), k recovered in the last stage
+    ("meq_rk4_u1", 0): 16, ("meq_rk4_u2", 0): 24, ("meq_rk4_u3", 0): 24, ("meq_rk4_u4", 0): 40,
 }
-STEP_BYTES = {(1, 0): 88, (1, 1): 56, (0, 0): 16}
+STEP_BYTES = {(1, 0): 88, (1, 1): 56, (0, 0): 16, (1, 0, "timevar"): 104}
 
 
 def config_rates(n, seed=1):
@@ -58,6 +60,19 @@ def config_rates(n, seed=1):
     a, b = rng.uniform(0.1, 1.0, 2)
     hops = np.clip(rng.lognormal(0.0, 0.5, n - 1), 0.1, 5.0)
     return np.concatenate([[a], hops, [b]])
+
+
+def config_timevar(n, seed=1):
+    """The time-variant run on the same lattice: r_i(t) = r_i (1 + 0.5 sin(w_i t)),
+    w_i ~ U[0.5, 2] drawn after the rates from the same stream, in the
+    reference's function form A sin(w t + phi) + c (src/lib/matvec.c:44-68)."""
+    rng = np.random.default_rng(seed)
+    rng.uniform(0.1, 1.0, 2)
+    rng.lognormal(0.0, 0.5, n - 1)
+    w = rng.uniform(0.5, 2.0, n + 1)
+    r = config_rates(n, seed)
+    return {"type": np.zeros(n + 1, dtype=np.int32), "amplitude": 0.5 * r, "period": w,
+            "offset": np.zeros(n + 1), "constant": r}
 
 
 def peaks():
@@ -265,6 +280,9 @@ def run_ours(args):
     N = 1 << n
     m = T.Meq(n, integ, prec, device=local)
     m.set_rates(rates)
+    tv = config_timevar(n) if args.timevar else None
+    if tv is not None:
+        m.set_timevar(tv["type"], tv["amplitude"], tv["period"], tv["offset"], tv["constant"])
     m.init(T.INIT_EMPTY)
     policy = m.cache_policy()
     stream = torch.cuda.ExternalStream(m.stream)
@@ -342,7 +360,7 @@ def run_ours(args):
                 "kernel_frac": {k: ALG_BYTES.get((k, prec), 0) * N / (v / 1000.0) / 1e9 / peak
                                 for k, v in kernel_ms.items()}}
     launches = int(sum(v[1] for v in prof.values()))
-    step_alg = STEP_BYTES.get((integ, prec), 0) * N
+    step_alg = STEP_BYTES.get((integ, prec, "timevar") if args.timevar else (integ, prec), 0) * N
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_sample(n, rates, h)
@@ -356,6 +374,8 @@ def run_ours(args):
         "config": {"workload": f"n={n}: 2^{n} states, seed-1 inhomogeneous rates, h=0.01, empty start; "
                                f"{'classical RK4' if integ else 'reference step'}",
                    "n": n, "integrator": args.integrator, "precision": args.precision,
+                   "rates": "time-variant r_i(t) = r_i (1 + 0.5 sin(w_i t)), w_i ~ U[0.5, 2], seed 1"
+                            if args.timevar else "constant",
                    "replicas": world, "l2": "inputs larger than L2 (8*2^n bytes per vector)",
                    "l2_policy": {"near_bits": policy[0], "flags": policy[1]},
                    "hbm_step_bytes_algorithmic": step_alg,
@@ -383,6 +403,8 @@ def main():
     ap.add_argument("--n", type=int, default=28, help="lattice length (the benchmark is n=28)")
     ap.add_argument("--integrator", choices=["rk4", "ref"], default="rk4")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--timevar", action="store_true",
+                    help="the time-variant run of the same lattice (RK4, FP64; rates evaluated per stage)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
