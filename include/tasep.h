@@ -132,6 +132,21 @@ typedef void (*tasep_snapshot_fn)(tasep_meq *m, uint64_t step, double t, void *u
 tasep_status tasep_meq_run_snapshots(tasep_meq *m, const tasep_run_config *rc, uint64_t every,
                                      tasep_snapshot_fn fn, void *user, tasep_run_result *res);
 
+/* The same snapshots without stopping the integration: each snapshot's
+ * observables (and, when with_probs is set, a copy of its 2^n probabilities)
+ * are taken on the device in stream order into one of two slots and copied to
+ * pinned host memory on a second stream while the steps go on; the loop reads
+ * its exit state one chunk behind the device.  fn gets, in step order, host
+ * pointers that are valid during the call only: rho[n] (bit order), cov[n*n]
+ * and mul[n*n] (site order), window4[(n-3)*16] (NULL for n < 4), as from
+ * tasep_meq_observables, and probs[2^n] (NULL unless with_probs).  Snapshots
+ * whose step the loop did not reach are not delivered.  fn must not call the
+ * handle.  Result and final state as tasep_meq_run_snapshots. */
+typedef void (*tasep_stream_fn)(tasep_meq *m, uint64_t step, double t, const double *rho, const double *cov,
+                                const double *mul, const double *window4, const double *probs, void *user);
+tasep_status tasep_meq_run_stream(tasep_meq *m, const tasep_run_config *rc, uint64_t every, int with_probs,
+                                  tasep_stream_fn fn, void *user, tasep_run_result *res);
+
 /* Enqueues `steps` steps on the handle's stream without the exit rule and
  * without waiting (benchmarks, CUDA-graph capture); t advances by h. */
 tasep_status tasep_meq_enqueue_steps(tasep_meq *m, double t0, double h, uint64_t steps);

@@ -39,7 +39,7 @@ EXPORTS = (
     "tasep_mlp_create", "tasep_mlp_destroy", "tasep_mlp_set_params", "tasep_mlp_get_params", "tasep_mlp_loss_grad",
     "tasep_mlp_train", "tasep_mlp_predict", "tasep_meq_init_pair_markov", "tasep_meq_run_snapshots",
     "tasep_meq_set_cache_policy", "tasep_meq_get_cache_policy", "tasep_test_inject_wait_expiry",
-    "tasep_batch_last_config",
+    "tasep_batch_last_config", "tasep_meq_run_stream",
 )
 
 
@@ -202,6 +202,41 @@ class Meq:
         rc = _RunCfg(t0, h, steps, stop_tol, stop_count, int(bool(exit_rule)))
         res = RunResult()
         _check(L.tasep_meq_run_snapshots(self._h, C.byref(rc), every, cb, None, C.byref(res)))
+        if errors:
+            raise errors[0]
+        return res.as_dict()
+
+    def run_stream(self, h, steps, every, fn, with_probs=False, t0=0.0, stop_tol=1e-10, stop_count=100,
+                   exit_rule=True):
+        """run() with snapshots that do not stop the integration: fn(step, t, obs, probs) for every step
+        whose index is a multiple of `every`, in step order, with obs a dict of copies of rho (bit
+        order), cov and mul (site order) and window4 ((n-3, 16), n >= 4), and probs a copy of the
+        2^n probabilities (None unless with_probs)."""
+        L = lib()
+        P = C.POINTER(C.c_double)
+        hook_t = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, P, P, P, P, P, C.c_void_p)
+        L.tasep_meq_run_stream.argtypes = [C.c_void_p, C.POINTER(_RunCfg), C.c_uint64, C.c_int, hook_t,
+                                           C.c_void_p, C.POINTER(RunResult)]
+        n, errors = self.n, []
+
+        def arr(p, k):
+            return np.ctypeslib.as_array(p, (k,)).copy() if p else None
+
+        def hook(_h, step, t, rho, cov, mul, w4, probs, _u):
+            try:
+                obs = {"rho": arr(rho, n), "cov": arr(cov, n * n).reshape(n, n),
+                       "mul": arr(mul, n * n).reshape(n, n)}
+                if n >= 4:
+                    obs["window4"] = arr(w4, (n - 3) * 16).reshape(n - 3, 16)
+                fn(step, t, obs, arr(probs, 1 << n))
+            except Exception as e:  # an exception cannot cross the C frame
+                errors.append(e)
+
+        cb = hook_t(hook)
+        rc = _RunCfg(t0, h, steps, stop_tol, stop_count, int(bool(exit_rule)))
+        res = RunResult()
+        _check(L.tasep_meq_run_stream(self._h, C.byref(rc), every, int(bool(with_probs)), cb, None,
+                                      C.byref(res)))
         if errors:
             raise errors[0]
         return res.as_dict()

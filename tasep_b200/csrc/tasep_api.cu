@@ -639,11 +639,12 @@ tasep_status tasep_meq_synchronize(tasep_meq *m) {
     return TASEP_OK;
 }
 
-tasep_status tasep_meq_observables(tasep_meq *m, double *rho, double *cov, double *mul, double *window4,
-                                   double *mass) {
-    if (!valid_handle(m)) return fail(TASEP_ERR_INVALID, "null handle");
-    if (!m->state_set) return fail(TASEP_ERR_INVALID, "initial state not set");
-    CU_TRY(cudaSetDevice(m->device));
+}  // extern "C"
+
+namespace {
+
+// Enqueues the observables of X[cur] into out (obs_count(n) raw sums).
+tasep_status obs_enqueue(tasep_meq *m, double *out, cudaStream_t st) {
     const int n = m->n, na = obs_count(n);
     static std::atomic<bool> configured[64] = {};
     if (!configured[m->device & 63].load(std::memory_order_acquire)) {
@@ -652,16 +653,16 @@ tasep_status tasep_meq_observables(tasep_meq *m, double *rho, double *cov, doubl
         configured[m->device & 63].store(true, std::memory_order_release);
     }
     ObsParams op{n, m->X[m->cur], m->obs_part};
-    tasep_status s = prof_begin(m, ST_COUNT + 1);
-    if (s) return s;
-    meq_obs_kernel<<<m->obs_rows, kObsThreads, obs_smem_bytes(n), m->stream>>>(op);
+    meq_obs_kernel<<<m->obs_rows, kObsThreads, obs_smem_bytes(n), st>>>(op);
     CU_TRY(cudaGetLastError());
-    meq_obs_reduce<<<(na + 255) / 256, 256, 0, m->stream>>>(m->obs_part, m->obs_rows, na, m->obs_out);
+    meq_obs_reduce<<<(na + 255) / 256, 256, 0, st>>>(m->obs_part, m->obs_rows, na, out);
     CU_TRY(cudaGetLastError());
-    if ((s = prof_end(m))) return s;
-    std::vector<double> o(na);
-    CU_TRY(cudaMemcpyAsync(o.data(), m->obs_out, sizeof(double) * na, cudaMemcpyDeviceToHost, m->stream));
-    CU_TRY(cudaStreamSynchronize(m->stream));
+    return TASEP_OK;
+}
+
+// Raw sums (total, second moments, 4-bit window marginals) to the outputs of
+// tasep_meq_observables.
+void obs_convert(int n, const double *o, double *rho, double *cov, double *mul, double *window4, double *mass) {
     const double S0 = o[0];
     std::vector<double> y(n);
     for (int a = 0; a < n; ++a) y[a] = o[obs_tri(n, a, a)];
@@ -682,6 +683,168 @@ tasep_status tasep_meq_observables(tasep_meq *m, double *rho, double *cov, doubl
     if (window4 && n >= 4)
         for (int p = 0; p + 4 <= n; ++p)
             for (int q = 0; q < 16; ++q) window4[p * 16 + q] = o[obs_p4(n, p, q)];
+}
+
+}  // namespace
+
+extern "C" {
+
+tasep_status tasep_meq_observables(tasep_meq *m, double *rho, double *cov, double *mul, double *window4,
+                                   double *mass) {
+    if (!valid_handle(m)) return fail(TASEP_ERR_INVALID, "null handle");
+    if (!m->state_set) return fail(TASEP_ERR_INVALID, "initial state not set");
+    CU_TRY(cudaSetDevice(m->device));
+    const int na = obs_count(m->n);
+    tasep_status s = prof_begin(m, ST_COUNT + 1);
+    if (s) return s;
+    if ((s = obs_enqueue(m, m->obs_out, m->stream))) return s;
+    if ((s = prof_end(m))) return s;
+    std::vector<double> o(na);
+    CU_TRY(cudaMemcpyAsync(o.data(), m->obs_out, sizeof(double) * na, cudaMemcpyDeviceToHost, m->stream));
+    CU_TRY(cudaStreamSynchronize(m->stream));
+    obs_convert(m->n, o.data(), rho, cov, mul, window4, mass);
+    return TASEP_OK;
+}
+
+tasep_status tasep_meq_run_stream(tasep_meq *m, const tasep_run_config *rc, uint64_t every, int with_probs,
+                                  tasep_stream_fn fn, void *user, tasep_run_result *res) {
+    if (!valid_handle(m) || !rc || !res || !fn || every < 1) return fail(TASEP_ERR_INVALID, "bad argument");
+    tasep_status s = check_ready(m, rc->h);
+    if (s) return s;
+    CU_TRY(cudaSetDevice(m->device));
+    memset(res, 0, sizeof *res);
+    constexpr int K = 2;  // snapshots in flight
+    const int n = m->n, na = obs_count(n);
+    const size_t pb = with_probs ? sizeof(double) * m->N : 0;
+    // device ring (observables, state copy, exit state per slot) and its pinned host mirror
+    struct Res {
+        double *d_obs = nullptr, *d_x = nullptr;
+        ExitState *d_ex = nullptr;
+        double *h_obs = nullptr, *h_x = nullptr;
+        ExitState *h_ex = nullptr, *h_chk = nullptr;
+        cudaStream_t main = nullptr, cp = nullptr;
+        cudaEvent_t ready[K] = {}, landed[K] = {}, chk[2] = {};
+        ~Res() {  // on every return: nothing in flight may still use the rings
+            if (main) cudaStreamSynchronize(main);
+            if (cp) cudaStreamSynchronize(cp);
+            cudaFree(d_obs); cudaFree(d_x); cudaFree(d_ex);
+            cudaFreeHost(h_obs); cudaFreeHost(h_x); cudaFreeHost(h_ex); cudaFreeHost(h_chk);
+            for (auto e : ready) if (e) cudaEventDestroy(e);
+            for (auto e : landed) if (e) cudaEventDestroy(e);
+            for (auto e : chk) if (e) cudaEventDestroy(e);
+            if (cp) cudaStreamDestroy(cp);
+        }
+    } r;
+    r.main = m->stream;
+    CU_TRY(cudaMalloc(&r.d_obs, sizeof(double) * na * K));
+    CU_TRY(cudaMalloc(&r.d_ex, sizeof(ExitState) * K));
+    CU_TRY(cudaMallocHost(&r.h_obs, sizeof(double) * na * K));
+    CU_TRY(cudaMallocHost(&r.h_ex, sizeof(ExitState) * K));
+    CU_TRY(cudaMallocHost(&r.h_chk, sizeof(ExitState) * 2));
+    if (pb) {
+        CU_TRY(cudaMalloc(&r.d_x, pb * K));
+        CU_TRY(cudaMallocHost(&r.h_x, pb * K));
+    }
+    CU_TRY(cudaStreamCreateWithFlags(&r.cp, cudaStreamNonBlocking));
+    for (int k = 0; k < K; ++k) {
+        CU_TRY(cudaEventCreateWithFlags(&r.ready[k], cudaEventDisableTiming));
+        CU_TRY(cudaEventCreateWithFlags(&r.landed[k], cudaEventDisableTiming));
+    }
+    for (auto &e : r.chk) CU_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    std::vector<double> rho(n), cov(size_t(n) * n), mul(size_t(n) * n), w4(n >= 4 ? (n - 3) * 16 : 1);
+    struct Snap { int slot; uint64_t step; double t; };
+    std::vector<Snap> queue;  // taken, not yet delivered (oldest first)
+    bool stopped = false;     // a delivered snapshot showed the loop had ended before it
+    auto deliver_oldest = [&]() -> tasep_status {
+        const Snap sn = queue.front();
+        queue.erase(queue.begin());
+        CU_TRY(cudaEventSynchronize(r.landed[sn.slot]));
+        const ExitState &e = r.h_ex[sn.slot];
+        if (e.error) return fail(TASEP_ERR_TIMEOUT, "a bounded device wait expired during the integration");
+        if (stopped || e.steps_done <= sn.step) {  // the loop ended before this step
+            stopped = true;
+            return TASEP_OK;
+        }
+        obs_convert(n, r.h_obs + size_t(sn.slot) * na, rho.data(), cov.data(), mul.data(), n >= 4 ? w4.data() : nullptr,
+                    nullptr);
+        fn(m, sn.step, sn.t, rho.data(), cov.data(), mul.data(), n >= 4 ? w4.data() : nullptr,
+           pb ? r.h_x + size_t(sn.slot) * m->N : nullptr, user);
+        return TASEP_OK;
+    };
+    const double thresh = rc->stop_tol * rc->h;
+    CU_TRY(cudaMemsetAsync(m->ex, 0, sizeof(ExitState), m->stream));
+    const int cur0 = m->cur;
+    const bool small = m->n <= kSmallMaxN;
+    const int shift = 30 - m->n;
+    const unsigned long long chunk = shift >= 10 ? 1024ull : (shift <= 2 ? 4ull : (1ull << shift));
+    double t = rc->t0;
+    unsigned long long i = 0, nsnap = 0, nchunk = 0;
+    while (i < rc->steps) {
+        // the exit state two chunks back tells whether to go on (one chunk of lookahead)
+        if (nchunk >= 2) {
+            CU_TRY(cudaEventSynchronize(r.chk[nchunk & 1]));
+            const ExitState &e = r.h_chk[nchunk & 1];
+            if (e.error) return fail(TASEP_ERR_TIMEOUT, "a bounded device wait expired during the integration");
+            if (e.done) break;
+        }
+        const unsigned long long snap = (i + every - 1) / every * every;
+        unsigned long long last = std::min<unsigned long long>(snap, rc->steps - 1);
+        if (!small) last = std::min(last, i + chunk - 1);
+        if (small) {
+            if ((s = small_run(m, t, rc->h, last - i + 1, i, thresh, rc->stop_count, rc->exit_rule))) return s;
+            for (unsigned long long j = i; j <= last; ++j) t += rc->h;
+        } else {
+            for (unsigned long long j = i; j <= last; ++j) {
+                if ((s = enqueue_step(m, j, t, rc->h, thresh, rc->stop_count, rc->exit_rule))) return s;
+                t += rc->h;
+            }
+        }
+        i = last + 1;
+        if (last % every == 0) {  // snapshot of step `last`, taken on the device in order
+            if (queue.size() == size_t(K) && (s = deliver_oldest())) return s;
+            const int slot = int(nsnap % K);
+            if ((s = obs_enqueue(m, r.d_obs + size_t(slot) * na, m->stream))) return s;
+            if (pb)
+                CU_TRY(cudaMemcpyAsync(r.d_x + size_t(slot) * m->N, m->X[m->cur], pb, cudaMemcpyDeviceToDevice,
+                                       m->stream));
+            CU_TRY(cudaMemcpyAsync(r.d_ex + slot, m->ex, sizeof(ExitState), cudaMemcpyDeviceToDevice, m->stream));
+            CU_TRY(cudaEventRecord(r.ready[slot], m->stream));
+            // to the host on the copy stream, while the integration goes on
+            CU_TRY(cudaStreamWaitEvent(r.cp, r.ready[slot], 0));
+            CU_TRY(cudaMemcpyAsync(r.h_obs + size_t(slot) * na, r.d_obs + size_t(slot) * na, sizeof(double) * na,
+                                   cudaMemcpyDeviceToHost, r.cp));
+            CU_TRY(cudaMemcpyAsync(r.h_ex + slot, r.d_ex + slot, sizeof(ExitState), cudaMemcpyDeviceToHost, r.cp));
+            if (pb)
+                CU_TRY(cudaMemcpyAsync(r.h_x + size_t(slot) * m->N, r.d_x + size_t(slot) * m->N, pb,
+                                       cudaMemcpyDeviceToHost, r.cp));
+            CU_TRY(cudaEventRecord(r.landed[slot], r.cp));
+            queue.push_back({slot, last, t});
+            ++nsnap;
+        }
+        CU_TRY(cudaMemcpyAsync(r.h_chk + (nchunk & 1), m->ex, sizeof(ExitState), cudaMemcpyDeviceToHost, m->stream));
+        CU_TRY(cudaEventRecord(r.chk[nchunk & 1], m->stream));
+        ++nchunk;
+        // hand over snapshots that have landed, without waiting for the others
+        while (!queue.empty() && cudaEventQuery(r.landed[queue.front().slot]) == cudaSuccess)
+            if ((s = deliver_oldest())) return s;
+    }
+    CU_TRY(cudaStreamSynchronize(m->stream));
+    while (!queue.empty())
+        if ((s = deliver_oldest())) return s;
+    if (m->prof && (s = prof_flush(m))) return s;
+    CU_TRY(cudaMemcpy(m->ex_host, m->ex, sizeof(ExitState), cudaMemcpyDeviceToHost));
+    const ExitState &e = *m->ex_host;
+    if (e.error) return fail(TASEP_ERR_TIMEOUT, "a bounded device wait expired during the integration");
+    const unsigned long long done = e.steps_done;
+    if (m->integrator == TASEP_INTEGRATOR_REF && !small) m->cur = int((cur0 + done) & 1ull);
+    res->steps_done = done;
+    res->steps_at_stop = e.steps_at_stop;
+    res->early_stop = e.early_stop;
+    res->converged = e.converged;
+    res->last_checksum = e.last_checksum;
+    double tt = rc->t0;
+    for (unsigned long long k = 0; k < done; ++k) tt += rc->h;
+    res->t_end = tt;
     return TASEP_OK;
 }
 

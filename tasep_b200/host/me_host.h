@@ -43,7 +43,6 @@ typedef struct {
     me_obs *obs;   /* count entries */
     double *probs; /* count * dim when keep_probs */
     double *corr;  /* count * (n - 5) */
-    double *buf;   /* dim doubles of scratch */
 } me_snaps;
 
 /* high_order_corr (src/masterEquation.c:47-75) evaluated on a full state

@@ -125,11 +125,13 @@ static int read_prob_file(const char *path, int n, double *x) {
     return seen == dim ? 0 : -2;
 }
 
-/* Snapshot of -a (src/masterEquation.c:646-666): densities, covariance and
- * product matrices from the device, the state itself for the 4-site
- * correlations of the timed correlation file and, when probabilities are
- * saved, for the probability snapshot file. */
-static void snapshot_hook(tasep_meq *m, uint64_t step, double t, void *user) {
+/* Snapshot of -a (src/masterEquation.c:646-666), streamed from the device
+ * while the integration goes on: densities, covariance and product matrices,
+ * and the state itself for the 4-site correlations of the timed correlation
+ * file and, when probabilities are saved, for the probability snapshot file. */
+static void snapshot_hook(tasep_meq *m, uint64_t step, double t, const double *rho, const double *cov,
+                          const double *mul, const double *window4, const double *probs, void *user) {
+    (void)m;
     (void)step;
     (void)t;
     me_snaps *s = (me_snaps *)user;
@@ -145,12 +147,12 @@ static void snapshot_hook(tasep_meq *m, uint64_t step, double t, void *user) {
     me_obs *ob = &s->obs[s->count];
     memset(ob, 0, sizeof *ob);
     ob->n = n;
-    double mass = 0;
-    if (tasep_meq_observables(m, ob->y, ob->cov, ob->mul, n >= 4 ? ob->p4 : NULL, &mass) != TASEP_OK)
-        tasep_fail("snapshot observables");
-    if (tasep_meq_store(m, s->buf, 0, s->dim) != TASEP_OK) tasep_fail("snapshot copy");
-    for (int k = 1; k <= vals; k++) s->corr[s->count * vals + (k - 1)] = me_state_corr(s->buf, n, 15, 4, n - 4 - k);
-    if (s->keep_probs) memcpy(s->probs + s->count * s->dim, s->buf, sizeof(double) * s->dim);
+    memcpy(ob->y, rho, sizeof(double) * n);
+    memcpy(ob->cov, cov, sizeof(double) * n * n);
+    memcpy(ob->mul, mul, sizeof(double) * n * n);
+    if (window4) memcpy(ob->p4, window4, sizeof(double) * (n - 3) * 16);
+    for (int k = 1; k <= vals; k++) s->corr[s->count * vals + (k - 1)] = me_state_corr(probs, n, 15, 4, n - 4 - k);
+    if (s->keep_probs) memcpy(s->probs + s->count * s->dim, probs, sizeof(double) * s->dim);
     s->count++;
 }
 
@@ -476,10 +478,8 @@ int main(int argc, char *argv[]) {
             snaps.n = n;
             snaps.dim = dim;
             snaps.keep_probs = save_p;
-            snaps.buf = (double *)malloc(sizeof(double) * dim);
-            if (snaps.buf == NULL) me_err_exit("ERROR: Not Enough memory to allocate animation data array", -1);
-            if (tasep_meq_run_snapshots(m, &rc, (uint64_t)animation_resolution, snapshot_hook, &snaps, &rr) !=
-                TASEP_OK)
+            if (tasep_meq_run_stream(m, &rc, (uint64_t)animation_resolution, n > 5 || save_p, snapshot_hook,
+                                     &snaps, &rr) != TASEP_OK)
                 tasep_fail("integration");
         } else if (tasep_meq_run(m, &rc, &rr) != TASEP_OK) {
             tasep_fail("integration");
@@ -567,7 +567,6 @@ int main(int argc, char *argv[]) {
         free(snaps.obs);
         free(snaps.probs);
         free(snaps.corr);
-        free(snaps.buf);
     }
 
     free(x);

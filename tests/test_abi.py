@@ -70,6 +70,11 @@ def test_sweep_and_warm_start_entry_points_validate_arguments():
     hook_t = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, C.c_void_p)
     L.tasep_meq_run_snapshots.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, hook_t, C.c_void_p, C.c_void_p]
     assert L.tasep_meq_run_snapshots(None, None, 1, hook_t(lambda *a: None), None, None) == 1
+    P = C.POINTER(C.c_double)
+    stream_t = C.CFUNCTYPE(None, C.c_void_p, C.c_uint64, C.c_double, P, P, P, P, P, C.c_void_p)
+    L.tasep_meq_run_stream.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int, stream_t, C.c_void_p,
+                                       C.c_void_p]
+    assert L.tasep_meq_run_stream(None, None, 1, 0, stream_t(lambda *a: None), None, None) == 1
     assert b"" != L.tasep_last_error()
 
 

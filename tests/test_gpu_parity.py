@@ -345,6 +345,58 @@ def test_run_snapshots_stop_at_the_exit_rule(n):
     assert steps == list(range(0, last + 1, 7))
 
 
+@pytest.mark.parametrize("n,integrator", [(9, T.INTEGRATOR_REF), (14, T.INTEGRATOR_RK4), (21, T.INTEGRATOR_REF),
+                                          (21, T.INTEGRATOR_RK4)])
+def test_run_stream_matches_run_snapshots(n, integrator):
+    """tasep_meq_run_stream: the snapshots streamed to the host while the steps
+    go on equal, bit for bit, the state and observables that the stopping
+    snapshot loop sees at the same steps, and the run ends in the same state."""
+    r = rates_for(n, 170 + n)
+    seen, streamed = [], []
+
+    def at_stop(mm, step, t):
+        seen.append((step, t, mm.store(), mm.observables()))
+
+    with T.Meq(n, integrator) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res = m.run_snapshots(0.01, 450, 50, at_stop)
+        x = m.store()
+    with T.Meq(n, integrator) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res2 = m.run_stream(0.01, 450, 50, lambda step, t, obs, probs: streamed.append((step, t, probs, obs)),
+                            with_probs=True)
+        assert np.array_equal(m.store(), x) and res2 == res
+    assert [s[0] for s in streamed] == [s[0] for s in seen] == list(range(0, 450, 50))
+    for (s1, t1, x1, o1), (s2, t2, x2, o2) in zip(seen, streamed):
+        assert t1 == t2 and np.array_equal(x1, x2)
+        for k in ("rho", "cov", "mul", "window4"):
+            assert np.array_equal(o1[k], o2[k]), k
+
+
+@pytest.mark.parametrize("n", [8, 19])
+def test_run_stream_stops_at_the_exit_rule(n):
+    """The streamed loop reads the exit state one chunk behind the device;
+    the steps it runs past the exit are no-ops and their snapshots are not
+    delivered."""
+    r = rates_for(n, 190 + n)
+    a, b = [], []
+    with T.Meq(n, T.INTEGRATOR_REF) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res = m.run_snapshots(0.01, 100000, 7, lambda mm, step, t: a.append(step), stop_tol=1e-4)
+        x = m.store()
+    with T.Meq(n, T.INTEGRATOR_REF) as m:
+        m.set_rates(r)
+        m.init(T.INIT_EMPTY)
+        res2 = m.run_stream(0.01, 100000, 7, lambda step, t, obs, probs: b.append((step, probs)), stop_tol=1e-4)
+        assert np.array_equal(m.store(), x)
+    assert res == res2 and res["converged"] == 1
+    assert [s for s, _ in b] == a == list(range(0, res["steps_done"], 7))
+    assert all(p is None for _, p in b)
+
+
 def test_timevar_rk4_many_tiles_per_cta():
     """Time-variant classical RK4 (stage kernels U1..U4, rates evaluated on the
     device at t, t+h/2, t+h/2, t+h) at n=23: 4096 tiles, every partner ring slot
