@@ -105,3 +105,23 @@ def test_learned_start_gains_over_cold_and_meanfield_starts():
     assert sum(r["learned"]["steps"] for r in rows) < sum(r["empty"]["steps"] for r in rows)
     assert np.median([r["prediction_density_err"] for r in rows]) < np.median(
         [r["meanfield_density_err"] for r in rows])
+
+
+def test_shipped_network_cuts_wall_time_to_the_exit_rule():
+    """The network shipped with the package (trained on n = 12..20) on held-out
+    rate vectors at n = 16: the measured wall time to the exit rule, network,
+    pair-Markov measure and run included, is at least 1.08x shorter than from
+    the empty lattice in total (1.20x measured on 64 vectors at n = 20), and
+    each run ends at the empty start's steady state."""
+    m = ws.pretrained()
+    try:
+        rows = ws.evaluate(m, 16, 12, seed=4, starts=("empty", "learned"))
+    finally:
+        m.close()
+    print(ws.summarize(rows, starts=("empty", "learned")))
+    for r in rows:
+        assert r["empty"]["converged"] and r["learned"]["converged"] and r["learned"]["start"] == "learned"
+        assert r["learned"]["max_density_diff"] < 1e-7
+    empty = sum(r["empty"]["seconds"] for r in rows)
+    learned = sum(r["learned"]["seconds"] for r in rows)
+    assert empty / learned > 1.08, (empty, learned)
