@@ -89,6 +89,9 @@ __global__ void __launch_bounds__(kSmallThreads, 1) meq_small_kernel(const __gri
     double *V2 = V1 + N;
     double *V3 = V2 + N;
     const int tid = threadIdx.x;
+    // a run whose exit rule already fired in an earlier launch (the host
+    // enqueues ahead of the exit state it has read) leaves the state as it is
+    if (p.mode == SM_RUN && *reinterpret_cast<volatile int *>(&p.ex->done)) return;
 
     for (uint32_t i = tid; i < N; i += kSmallThreads) X[i] = p.x_in[i];
     if (tid == 0) *flag = 0;
