@@ -102,20 +102,20 @@ __global__ void batch_compact_kernel(const BatchExit *ex, int nsys, int *list, i
 
 // k-th tile of this CTA's sequence, as a global tile index (ntiles when past
 // the end).  Only systems on the running list are visited.
-__device__ __forceinline__ unsigned long long batch_tile(const BatchParams &p, unsigned long long k, int ntb,
-                                                         unsigned long long ntiles, int na) {
-    const unsigned long long mask = (1ull << ntb) - 1;
-    unsigned long long e, t;
+// Tile indices are 32-bit (the host keeps nsys * tiles per system below 2^31).
+__device__ __forceinline__ uint32_t batch_tile(const BatchParams &p, uint32_t k, int ntb, uint32_t ntiles, int na) {
+    const uint32_t mask = (1u << ntb) - 1;
+    uint32_t e, t;
     if (!p.sys_major) {
-        const unsigned long long l = blockIdx.x + k * gridDim.x;
+        const uint32_t l = blockIdx.x + k * gridDim.x;
         e = l >> ntb;
         t = l & mask;
     } else {
         e = blockIdx.x + (k >> ntb) * gridDim.x;
         t = k & mask;
     }
-    if (e >= (unsigned long long)na) return ntiles;
-    return ((unsigned long long)p.list[e] << ntb) | t;
+    if (e >= uint32_t(na)) return ntiles;
+    return (uint32_t(p.list[e]) << ntb) | t;
 }
 
 template <typename G> __device__ __forceinline__ G batch_rate(const double *r, int i) {
@@ -145,8 +145,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
     const int warp = tid >> 5, lane = tid & 31;
     const int n = p.n;
     const int ntb = p.tps_bits;  // tile bits inside a system (>= 1)
-    const unsigned long long tps = 1ull << ntb;
-    const unsigned long long ntiles = (unsigned long long)p.nsys << ntb;
+    const uint32_t tps = 1u << ntb;
+    const uint32_t ntiles = uint32_t(p.nsys) << ntb;
     const int R = n + 1;
     const int na = *p.count;  // running systems this step (set before the launch)
 
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
     }
     __syncthreads();
     volatile int *errf = &c.err;
-    const unsigned long long lowmask = ntb >= 2 ? ((1ull << (ntb - 1)) - 1) : 0ull;
+    const uint32_t lowmask = ntb >= 2 ? ((1u << (ntb - 1)) - 1) : 0u;
     const G *__restrict__ g = static_cast<const G *>(p.g);
 
     if (warp == kConsumerWarps) {
@@ -176,20 +176,20 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
             int pslot = 0;
             uint32_t plap = 0;
             bool ok = true;
-            for (unsigned long long k = 0; ok; ++k) {
-                const unsigned long long T = batch_tile(p, k, ntb, ntiles, na);
+            for (uint32_t k = 0; ok; ++k) {
+                const uint32_t T = batch_tile(p, k, ntb, ntiles, na);
                 if (T >= ntiles) break;
-                const unsigned long long t = T & (tps - 1), base = T - t;
+                const uint32_t t = T & (tps - 1), base = T - t;
                 const int b = it & 1;
                 if (it >= 2 && !mbar_wait(&c.empty[b], ((it >> 1) - 1) & 1, errf)) break;
                 unsigned char *st = stage_base + b * gb;
                 mbar_arrive_expect_tx(&c.full[b], gb);
-                bulk_g2s(st, g + T * kTile, gb, &c.full[b], normal);
+                bulk_g2s(st, g + (unsigned long long)T * kTile, gb, &c.full[b], normal);
                 const bool top = (t >> (ntb - 1)) & 1;
                 const bool strad = !(t & 1);
-                const unsigned long long hmask = t & ~(t >> 1) & lowmask;
-                const int np = int(top) + int(strad) + __popcll(hmask);
-                unsigned long long hm = hmask;
+                const uint32_t hmask = t & ~(t >> 1) & lowmask;
+                const int np = int(top) + int(strad) + __popc(hmask);
+                uint32_t hm = hmask;
                 for (int q = 0; q < np; ++q) {
                     unsigned long long src;
                     uint32_t bytes = gb;
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
                         src = t + 1;
                         bytes = gb / 2;
                     } else {
-                        const int u = __ffsll(hm) - 1;
+                        const int u = __ffs(hm) - 1;
                         hm &= hm - 1;
                         src = t + (1ull << u);
                     }
@@ -256,17 +256,17 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
     uint32_t cph = 0;
     bool ok = true;
 
-    for (unsigned long long k = 0;; ++k) {
-        const unsigned long long T = batch_tile(p, k, ntb, ntiles, na);
+    for (uint32_t k = 0;; ++k) {
+        const uint32_t T = batch_tile(p, k, ntb, ntiles, na);
         if (T >= ntiles) break;
-        const unsigned long long sys = T >> ntb, t = T & (tps - 1);
+        const uint32_t sys = T >> ntb, t = T & (tps - 1);
         const int b = it & 1;
         const bool top = (t >> (ntb - 1)) & 1;
         const bool strad = !(t & 1);
-        const unsigned long long hmask = t & ~(t >> 1) & lowmask;
-        const unsigned long long dhmask = ~t & (t >> 1) & lowmask;
-        const unsigned long long gT = T * kTile;
-        const double *rs = p.rates + sys * R;
+        const uint32_t hmask = t & ~(t >> 1) & lowmask;
+        const uint32_t dhmask = ~t & (t >> 1) & lowmask;
+        const unsigned long long gT = (unsigned long long)T * kTile;
+        const double *rs = p.rates + size_t(sys) * R;
         const G rn = batch_rate<G>(rs, n), r0 = batch_rate<G>(rs, 0), rn1 = batch_rate<G>(rs, n - 1);
         const G r9 = batch_rate<G>(rs, n - 10), rnL = batch_rate<G>(rs, n - kTileBits);
 
@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
         // low diagonal prefixes of this system
         G d0, d1, d2, d3;
         {
-            const G *dt = dtab_all + (sys * 2 + (top ? 1 : 0)) * kTile;
+            const G *dt = dtab_all + (size_t(sys) * 2 + (top ? 1 : 0)) * kTile;
             const G *q0 = dt + pb0, *q1 = dt + pb1;
             d0 = q0[0]; d1 = q0[1]; d2 = q1[0]; d3 = q1[1];
         }
@@ -309,8 +309,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
         if (!strad) { d0 -= rnL; d1 -= rnL; }
         {
             G ds = G(0);
-            for (unsigned long long mh = dhmask; mh; mh &= mh - 1)
-                ds += batch_rate<G>(rs, n - 1 - kTileBits - (__ffsll(mh) - 1));
+            for (uint32_t mh = dhmask; mh; mh &= mh - 1)
+                ds += batch_rate<G>(rs, n - 1 - kTileBits - (__ffs(mh) - 1));
             d0 -= ds; d1 -= ds; d2 -= ds; d3 -= ds;
         }
         a0 = fma(d0, x0, a0); a1 = fma(d1, x1, a1); a2 = fma(d2, x2, a2); a3 = fma(d3, x3, a3);
@@ -353,10 +353,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
             consumer_release(&c.rempty[cslot], lane);
             if (++cslot == RS) { cslot = 0; cph ^= 1; }
         }
-        for (unsigned long long mh = hmask; mh; mh &= mh - 1) {
+        for (uint32_t mh = hmask; mh; mh &= mh - 1) {
             if (!mbar_wait(&c.rfull[cslot], cph, errf)) { ok = false; break; }
             const G *pp = reinterpret_cast<const G *>(ring_base + cslot * gb);
-            const G rr = batch_rate<G>(rs, n - 1 - kTileBits - (__ffsll(mh) - 1));
+            const G rr = batch_rate<G>(rs, n - 1 - kTileBits - (__ffs(mh) - 1));
             G p0, p1, p2, p3;
             V2<G>::lds(pp + pb0, p0, p1);
             V2<G>::lds(pp + pb1, p2, p3);
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
             // this warp's share of the system's L1 norm goes to a fixed slot; the
             // system's last warp adds the slots in order and applies the exit rule
             const double ws = warp_sum(cs);
-            double *slots = p.partials + sys * (tps * kConsumerWarps);
+            double *slots = p.partials + size_t(sys) * (tps * kConsumerWarps);
             unsigned tk = 0;
             if (lane == 0) {
                 slots[t * kConsumerWarps + warp] = ws;

@@ -164,8 +164,8 @@ __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;"
 // other partners' sweep distances double, which moves one hop pair out of
 // the L2 window (a quarter of the tiles): 1.5 instead of 1.75 far-partner
 // reads per tile at n = 28.
-__device__ __forceinline__ unsigned long long sweep_tile(unsigned long long o, int ntb) {
-    return ntb >= 2 ? ((o >> 1) | ((o & 1ull) << (ntb - 1))) : o;
+__device__ __forceinline__ uint32_t sweep_tile(uint32_t o, int ntb) {
+    return ntb >= 2 ? ((o >> 1) | ((o & 1u) << (ntb - 1))) : o;
 }
 
 template <typename G> __device__ __forceinline__ G rate_of(const TileCtrl &c, int i);
@@ -198,6 +198,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     const int warp = tid >> 5, lane = tid & 31;
     const int n = p.n;
     const int ntb = n - kTileBits;  // tile-index bits (>= 1)
+    // tile indices fit 32 bits (at most 2^22 tiles for n <= 33); 32-bit masks
+    // and bit scans cost half the integer instructions of 64-bit ones
+    const uint32_t ntiles = uint32_t(p.ntiles);
 
     if (tid == 0) {
         c.skip = (p.skip_if_done && p.ex) ? *reinterpret_cast<volatile int *>(&p.ex->done) : 0;
@@ -237,8 +240,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             const bool skip_copy = kTuned && p.skip_copy_plus1 > 0 && blockIdx.x == 0;
             uint32_t it = 0, cur = 0;
             bool ok = true;
-            for (unsigned long long ord = blockIdx.x; ord < p.ntiles && ok; ord += gridDim.x, ++it) {
-                const unsigned long long T = sweep_tile(ord, ntb);
+            for (uint32_t ord = blockIdx.x; ord < ntiles && ok; ord += gridDim.x, ++it) {
+                const uint32_t T = sweep_tile(ord, ntb);
                 const int b = it & 1;
                 if (it >= 2 && !mbar_wait(&c.empty[b], ((it >> 1) - 1) & 1, errf, wait_ns)) break;
                 unsigned char *st = stage_base + b * LY::stage;
@@ -247,10 +250,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 // partner tiles, in the order the consumers add them
                 const bool top = (T >> (ntb - 1)) & 1;
                 const bool strad = !(T & 1);
-                const unsigned long long hmask =
-                    ntb >= 2 ? (T & ~(T >> 1) & ((1ull << (ntb - 1)) - 1)) : 0ull;
-                const int np = int(top) + int(strad) + __popcll(hmask);
-                unsigned long long hm = hmask;
+                const uint32_t hmask = ntb >= 2 ? (T & ~(T >> 1) & ((1u << (ntb - 1)) - 1)) : 0u;
+                const int np = int(top) + int(strad) + __popc(hmask);
+                uint32_t hm = hmask;
                 for (int q = 0; q < np; ++q) {
                     unsigned long long src;
                     uint32_t bytes = LY::gb;
@@ -262,7 +264,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                         src = T + 1;
                         bytes = LY::gb / 2;
                     } else {
-                        const int u = __ffsll(hm) - 1;
+                        const int u = __ffs(hm) - 1;
                         hm &= hm - 1;
                         src = T + (1ull << u);
                         if constexpr (kTuned)
@@ -349,15 +351,15 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     uint32_t cph = 0;  // its fill parity
     bool ok = true;
 
-    for (unsigned long long ord = blockIdx.x; ord < p.ntiles; ord += gridDim.x, ++it) {
-        const unsigned long long T = sweep_tile(ord, ntb);
+    for (uint32_t ord = blockIdx.x; ord < ntiles; ord += gridDim.x, ++it) {
+        const uint32_t T = sweep_tile(ord, ntb);
         const int b = it & 1;
         const bool top = (T >> (ntb - 1)) & 1;
         const bool strad = !(T & 1);
-        const unsigned long long lowmask = ntb >= 2 ? ((1ull << (ntb - 1)) - 1) : 0ull;
-        const unsigned long long hmask = T & ~(T >> 1) & lowmask;
-        const unsigned long long dhmask = ~T & (T >> 1) & lowmask;
-        const unsigned long long gT = T * kTile;
+        const uint32_t lowmask = ntb >= 2 ? ((1u << (ntb - 1)) - 1) : 0u;
+        const uint32_t hmask = T & ~(T >> 1) & lowmask;
+        const uint32_t dhmask = ~T & (T >> 1) & lowmask;
+        const unsigned long long gT = (unsigned long long)T * kTile;
 
         // per-state extra inputs, read once straight into registers; they are
         // only needed in the epilogue, so their latency hides behind the sweep
@@ -409,17 +411,17 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             d0 = A::sub(d0, rnL); d1 = A::sub(d1, rnL);
         }
         if constexpr (Tr::EXACT) {  // the reference's subtraction order
-            unsigned long long mh = dhmask;
+            uint32_t mh = dhmask;
             while (mh) {
-                const int u = __ffsll(mh) - 1;
+                const int u = __ffs(mh) - 1;
                 mh &= mh - 1;
                 const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 d0 = A::sub(d0, rr); d1 = A::sub(d1, rr); d2 = A::sub(d2, rr); d3 = A::sub(d3, rr);
             }
         } else {  // reassociation allowed: one sum of the tile-level rates
             G ds = G(0);
-            for (unsigned long long mh = dhmask; mh; mh &= mh - 1)
-                ds += rate_of<G>(c, n - 1 - kTileBits - (__ffsll(mh) - 1));
+            for (uint32_t mh = dhmask; mh; mh &= mh - 1)
+                ds += rate_of<G>(c, n - 1 - kTileBits - (__ffs(mh) - 1));
             d0 -= ds; d1 -= ds; d2 -= ds; d3 -= ds;
         }
         a0 = A::madd(a0, d0, x0); a1 = A::madd(a1, d1, x1);
@@ -479,9 +481,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             if (++cslot == RS) { cslot = 0; cph ^= 1; }
         }
         {
-            unsigned long long mh = hmask;  // k >= 11
+            uint32_t mh = hmask;  // k >= 11
             while (mh) {
-                const int u = __ffsll(mh) - 1;
+                const int u = __ffs(mh) - 1;
                 mh &= mh - 1;
                 const int slot = cslot;
                 if (!mbar_wait(&c.rfull[slot], cph, errf, wait_ns)) { ok = false; break; }

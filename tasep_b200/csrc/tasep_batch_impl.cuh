@@ -333,6 +333,8 @@ tasep_status tasep_batch_create(int n, int nsys, int precision, int device, void
     *out = nullptr;
     if (n <= kTileBits || n > 24) return fail(TASEP_ERR_INVALID, "batched systems need %d < n <= 24", kTileBits);
     if (nsys < 1) return fail(TASEP_ERR_INVALID, "nsys=%d", nsys);
+    if ((uint64_t(nsys) << (n - kTileBits)) >= (1ull << 31))  // 32-bit tile indices in the sweep
+        return fail(TASEP_ERR_INVALID, "nsys=%d systems of n=%d exceed 2^31 tiles", nsys, n);
     if (precision != TASEP_PRECISION_FP64 && precision != TASEP_PRECISION_MIXED)
         return fail(TASEP_ERR_INVALID, "unknown precision %d", precision);
     int ndev = 0;
