@@ -320,6 +320,10 @@ const char *tasep_last_error(void);
  * TASEP_ERR_TIMEOUT and their results are invalid.  (0, -1) switches the
  * hook off; it is process-wide and not meant for concurrent use. */
 tasep_status tasep_test_inject_wait_expiry(uint64_t wait_limit_ns, int skip_partner_copy);
+/* Test entry: out[i] = in[i] / 6 as the REF and time-variant steps compute it
+ * on the device (correctly rounded, without a division instruction sequence),
+ * for checking against IEEE division on the host. */
+tasep_status tasep_test_div6(const double *host_in, double *host_out, uint64_t count);
 int tasep_abi_version(void);
 /* Bytes of device memory a handle with this configuration allocates. */
 uint64_t tasep_meq_footprint(int n, int integrator, int precision, int timevar);

@@ -39,7 +39,7 @@ EXPORTS = (
     "tasep_mlp_create", "tasep_mlp_destroy", "tasep_mlp_set_params", "tasep_mlp_get_params", "tasep_mlp_loss_grad",
     "tasep_mlp_train", "tasep_mlp_predict", "tasep_meq_init_pair_markov", "tasep_meq_run_snapshots",
     "tasep_meq_set_cache_policy", "tasep_meq_get_cache_policy", "tasep_test_inject_wait_expiry",
-    "tasep_batch_last_config", "tasep_meq_run_stream",
+    "tasep_batch_last_config", "tasep_meq_run_stream", "tasep_test_div6",
 )
 
 
@@ -107,6 +107,7 @@ def lib():
         L.tasep_meq_set_cache_policy.argtypes = [H, C.c_int, C.c_int]
         L.tasep_meq_get_cache_policy.argtypes = [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]
         L.tasep_test_inject_wait_expiry.argtypes = [C.c_uint64, C.c_int]
+        L.tasep_test_div6.argtypes = [_dp, _dp, C.c_uint64]
         _lib = L
     return _lib
 
@@ -124,6 +125,14 @@ def inject_wait_expiry(wait_limit_ns=0, skip_partner_copy=-1):
     """Test hook: bounded device waits give up after wait_limit_ns and the first
     CTA leaves out one partner copy (see include/tasep.h); (0, -1) turns it off."""
     _check(lib().tasep_test_inject_wait_expiry(int(wait_limit_ns), int(skip_partner_copy)))
+
+
+def div6(x):
+    """Test entry: x / 6 as the device steps compute it (see include/tasep.h)."""
+    x = _f64(x).ravel()
+    out = np.empty_like(x)
+    _check(lib().tasep_test_div6(x.ctypes.data_as(_dp), out.ctypes.data_as(_dp), x.size))
+    return out
 
 
 def footprint(n, integrator=INTEGRATOR_RK4, precision=PRECISION_FP64, timevar=False):

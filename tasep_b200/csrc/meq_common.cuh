@@ -97,6 +97,29 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// RN(s / 6), the last operation of the reference's (k1 + 2 k2 + 2 k3 + k4) / 6
+// (src/lib/solv.c:44-52), without a division instruction sequence.  Markstein's
+// correction step (P. Markstein, IBM J. Res. Dev. 34(1), 1990): with
+// z = RN(1/6), q = RN(s z) is within one ulp of v = s/6 (z is within 2^-56 of
+// 1/6), the remainder r = s - 6q is exactly representable, so fma gives it
+// exactly, and q' = RN(q + r z) differs from RN(q + r/6) = RN(v) only if
+// q + r z and v straddle a rounding midpoint.  They cannot: |q + r z - v| =
+// |r| |z - 1/6| < 12 ulp(v) 2^-56, while for a 53-bit s = S 2^E the distance
+// from S 2^E / 6 to any midpoint of its binade is |8S - 3(2k+1)| 2^E / 48 or
+// |4S - 3(2k+1)| 2^E / 24, an odd multiple of at least 2^E / 48 >= ulp(v) / 12.
+// The argument needs s, q and r normal: 2^-900 <= |s| <= 2^1000; zeros,
+// subnormals, infinities and NaN take the IEEE division.
+__device__ __forceinline__ double div6_rn(double s) {
+    constexpr double z = 1.0 / 6.0;  // RN(1/6), folded by the compiler
+    const double a = fabs(s);
+    if (a >= 0x1p-900 && a <= 0x1p+1000) {
+        const double q = __dmul_rn(s, z);
+        const double r = __fma_rn(-q, 6.0, s);
+        return __fma_rn(r, z, q);
+    }
+    return __ddiv_rn(s, 6.0);
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(

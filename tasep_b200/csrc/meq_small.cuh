@@ -134,7 +134,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) meq_small_kernel(const __gri
             for (uint32_t i = tid; i < N; i += kSmallThreads) {
                 const double kv = __dmul_rn(h, small_row<double>(n, i, rd, X));
                 const double k2 = __dmul_rn(2.0, kv);
-                const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv), 6.0);
+                const double D = div6_rn(__dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv));
                 V1[i] = __dadd_rn(X[i], D);
                 cs += fabs(D);
             }
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1) meq_small_kernel(const __gri
                 const double x = X[i];
                 const double k1 = 2.0 * (V1[i] - x), k2 = 2.0 * (V2[i] - x), k3 = V3[i] - x;
                 const double k4 = __dmul_rn(h, small_row<double>(n, i, rd + 3 * kMaxR, V3));
-                const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4), 6.0);
+                const double D = div6_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4));
                 X[i] = __dadd_rn(x, D);
                 cs += fabs(D);
             }

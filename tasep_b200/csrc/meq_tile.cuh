@@ -512,7 +512,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             } else if constexpr (S == ST_REF) {
                 const double kv = __dmul_rn(p.h, Tv);
                 const double k2 = __dmul_rn(2.0, kv);
-                const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv), 6.0);
+                const double D = div6_rn(__dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv));
                 o[j] = __dadd_rn(xv[j], D);
                 cs += fabs(D);
             } else if constexpr (S == ST_H1) {
@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 const double k2 = 2.0 * (xc[j] - x);
                 const double k3 = xv[j] - x;
                 const double k4 = __dmul_rn(p.h, Tv);
-                const double D = __ddiv_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4), 6.0);
+                const double D = div6_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4));
                 o[j] = __dadd_rn(x, D);
                 cs += fabs(D);
             }

@@ -290,6 +290,12 @@ tasep_status small_run(tasep_meq *m, double t0, double h, unsigned long long ste
     return prof_end(m);
 }
 
+// The step's RN(s / 6) applied to a vector (tasep_test_div6).
+__global__ void div6_kernel(double *v, uint64_t count) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < count; i += uint64_t(gridDim.x) * blockDim.x)
+        v[i] = div6_rn(v[i]);
+}
+
 bool valid_handle(const tasep_meq *m) { return m != nullptr && m->n >= 1; }
 
 }  // namespace
@@ -304,6 +310,27 @@ tasep_status tasep_test_inject_wait_expiry(uint64_t wait_limit_ns, int skip_part
     g_test_skip_copy.store(skip_partner_copy + 1);
     return TASEP_OK;
 }
+tasep_status tasep_test_div6(const double *host_in, double *host_out, uint64_t count) {
+    if ((!host_in || !host_out) && count) return fail(TASEP_ERR_INVALID, "null argument");
+    if (count == 0) return TASEP_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(TASEP_ERR_NODEV, "no CUDA device");
+    }
+    double *d = nullptr;
+    CU_TRY(cudaMalloc(&d, sizeof(double) * count));
+    struct Free {
+        double *p;
+        ~Free() { cudaFree(p); }
+    } guard{d};
+    CU_TRY(cudaMemcpy(d, host_in, sizeof(double) * count, cudaMemcpyHostToDevice));
+    div6_kernel<<<unsigned((count + 255) / 256 < 65535 ? (count + 255) / 256 : 65535), 256>>>(d, count);
+    CU_TRY(cudaGetLastError());
+    CU_TRY(cudaMemcpy(host_out, d, sizeof(double) * count, cudaMemcpyDeviceToHost));
+    return TASEP_OK;
+}
+
 int tasep_abi_version(void) { return TASEP_ABI_VERSION; }
 
 uint64_t tasep_meq_footprint(int n, int integrator, int precision, int timevar) {
