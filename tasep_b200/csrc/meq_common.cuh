@@ -107,8 +107,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // |r| |z - 1/6| < 12 ulp(v) 2^-56, while for a 53-bit s = S 2^E the distance
 // from S 2^E / 6 to any midpoint of its binade is |8S - 3(2k+1)| 2^E / 48 or
 // |4S - 3(2k+1)| 2^E / 24, an odd multiple of at least 2^E / 48 >= ulp(v) / 12.
-// The argument needs s, q and r normal: 2^-900 <= |s| <= 2^1000; zeros,
-// subnormals, infinities and NaN take the IEEE division.
+// The argument needs s, q and r normal: 2^-900 <= |s| <= 2^1000.  Zeros (most
+// states early in a run from a pure state) are their own quotient; the rest
+// (subnormals, infinities, NaN) take the IEEE division.
 __device__ __forceinline__ double div6_rn(double s) {
     constexpr double z = 1.0 / 6.0;  // RN(1/6), folded by the compiler
     const double a = fabs(s);
@@ -117,6 +118,7 @@ __device__ __forceinline__ double div6_rn(double s) {
         const double r = __fma_rn(-q, 6.0, s);
         return __fma_rn(r, z, q);
     }
+    if (a == 0.0) return s;
     return __ddiv_rn(s, 6.0);
 }
 

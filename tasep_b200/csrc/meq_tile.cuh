@@ -147,10 +147,12 @@ template <int S, typename E> struct TileLayout {
     static constexpr int x2b = Tr::NX > 2 ? kTile * sizeof(typename Tr::X2) : 0;
     static constexpr int stage = gb;     // the gathered tile; extras go straight to registers
     static constexpr int dtab = 2 * gb;  // low diagonal prefixes, for top bit clear / set
+    // tile-level diagonal sums of the reassociating stages: 6 windows x 32 entries
+    static constexpr int dst = Tr::EXACT ? 0 : int(6 * 32 * sizeof(typename Tr::G));
     // as many partner slots as shared memory holds
-    static constexpr int RS0 = (kSmemMax - kCtrlBytes - 2 * stage - dtab) / gb;
+    static constexpr int RS0 = (kSmemMax - kCtrlBytes - 2 * stage - dtab - dst) / gb;
     static constexpr int RS = RS0 < kMaxRing ? RS0 : kMaxRing;
-    static constexpr int bytes = kCtrlBytes + 2 * stage + RS * gb + dtab;
+    static constexpr int bytes = kCtrlBytes + 2 * stage + RS * gb + dtab + dst;
     static_assert(RS >= 4, "partner ring too shallow");
 };
 
@@ -192,6 +194,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     unsigned char *stage_base = tile_smem + kCtrlBytes;
     unsigned char *ring_base = stage_base + 2 * LY::stage;
     G *dtab = reinterpret_cast<G *>(ring_base + LY::RS * LY::gb);
+    G *dst = dtab + 2 * kTile;  // reassociating stages only
     constexpr int RS = LY::RS;
 
     const int tid = threadIdx.x;
@@ -316,6 +319,23 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             dtab[tp * kTile + l] = d;
         }
     }
+    if constexpr (!Tr::EXACT) {
+        // Tile-level diagonal: the sum of r[n-1-11-u] over the tile-index
+        // pairs u with bit u clear and bit u+1 set, looked up in windows of
+        // five tile-index bits: window w covers u = 4w..4w+3, entry e holds
+        // the sum over those pairs that e's bits select.  Stages that must
+        // keep the reference's subtraction order run the loop below instead.
+        for (int l = tid; l < 6 * 32; l += kConsumers) {
+            const int w = l >> 5, e = l & 31;
+            G v = G(0);
+            for (int j = 0; j < 4; ++j) {
+                const int u = 4 * w + j;
+                if (u <= ntb - 2 && !((e >> j) & 1) && ((e >> (j + 1)) & 1)) v += rate_of<G>(c, n - 1 - kTileBits - u);
+            }
+            dst[l] = v;
+        }
+    }
+    const int nwin = (ntb + 2) / 4;  // windows holding a pair u <= ntb - 2
     const G rn = rate_of<G>(c, n), r0 = rate_of<G>(c, 0), rn1 = rate_of<G>(c, n - 1);
     const G r9 = rate_of<G>(c, n - 10), rnL = rate_of<G>(c, n - kTileBits);
     consumer_sync();
@@ -418,10 +438,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 const G rr = rate_of<G>(c, n - 1 - kTileBits - u);
                 d0 = A::sub(d0, rr); d1 = A::sub(d1, rr); d2 = A::sub(d2, rr); d3 = A::sub(d3, rr);
             }
-        } else {  // reassociation allowed: one sum of the tile-level rates
-            G ds = G(0);
-            for (uint32_t mh = dhmask; mh; mh &= mh - 1)
-                ds += rate_of<G>(c, n - 1 - kTileBits - (__ffs(mh) - 1));
+        } else {  // reassociation allowed: one sum of the tile-level rates, from the windows
+            G ds = dst[T & 31];
+#pragma unroll
+            for (int w = 1; w < 6; ++w)
+                if (w < nwin) ds += dst[w * 32 + ((T >> (4 * w)) & 31)];
             d0 -= ds; d1 -= ds; d2 -= ds; d3 -= ds;
         }
         a0 = A::madd(a0, d0, x0); a1 = A::madd(a1, d1, x1);
