@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 if (it >= 2 && !mbar_wait(&c.empty[b], ((it >> 1) - 1) & 1, errf, wait_ns)) break;
                 unsigned char *st = stage_base + b * LY::stage;
                 mbar_arrive_expect_tx(&c.full[b], LY::stage);
-                bulk_g2s(st, g + T * kTile, LY::gb, &c.full[b], own_pol);  // read again only as a far partner
+                bulk_g2s(st, g + (unsigned long long)T * kTile, LY::gb, &c.full[b], own_pol);  // read again only as a far partner
                 // partner tiles, in the order the consumers add them
                 const bool top = (T >> (ntb - 1)) & 1;
                 const bool strad = !(T & 1);
