@@ -42,7 +42,6 @@ struct BatchParams {
     void *out;
     double h, hc;
     const double *rates;      // [nsys][n+1]
-    const void *dtab;         // [nsys][2][kTile] low diagonal prefixes in the gather type
     double *partials;         // [nsys][tiles per system][kConsumerWarps]
     unsigned int *counters;   // [nsys]
     BatchExit *ex;            // [nsys]
@@ -56,23 +55,6 @@ struct BatchParams {
     int exit_rule;
     unsigned long long max_steps;
 };
-
-// Low diagonal prefixes of every system (same order as meq_tile.cuh).
-template <typename G>
-__global__ void batch_setup_kernel(int n, int nsys, const double *rates, G *dtab) {
-    const int R = n + 1;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)nsys * 2 * kTile;
-         e += (long long)gridDim.x * blockDim.x) {
-        const int sys = int(e / (2 * kTile)), tp = int((e / kTile) & 1), l = int(e % kTile);
-        const double *r = rates + (size_t)sys * R;
-        G d = G(0);
-        if (l & 1) d -= G(r[n]);
-        if (!tp) d -= G(r[0]);
-        for (int j = 0; j < kTileBits - 1; ++j)
-            if (!((l >> j) & 1) && ((l >> (j + 1)) & 1)) d -= G(r[n - 1 - j]);
-        dtab[e] = d;
-    }
-}
 
 // Rebuilds the list of running systems (ascending ids) after a step, so the
 // next step's launches visit only their tiles.  One CTA; ballot-based scan.
@@ -234,7 +216,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
     // ---------------- consumers (pair layout of meq_tile.cuh) ----------------
     const uint64_t once = policy_evict_first();
     O *__restrict__ out = static_cast<O *>(p.out);
-    const G *__restrict__ dtab_all = static_cast<const G *>(p.dtab);
     const uint32_t t9 = tid;
     const int pb0 = 2 * tid, pb1 = 2 * tid + kTile / 2;
     const bool b9 = (t9 >> 8) & 1;
@@ -251,6 +232,24 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
             qidx[k] = n - 2 - q;
         }
     }
+    // This thread's part of the diagonal below the tile level, in terms of the
+    // system's rates: the pairs j = 1..8 (state bits j, j+1 = t bits j-1, j)
+    // with b_j = 0, b_(j+1) = 1 are the same for its four states; j = 0 adds
+    // r[n-1] to the first state of each pair if t bit 0 is set; j = 9 adds
+    // r[n-10] to the P1 states (bit 10 set) if t bit 8 is clear; the exit term
+    // r[n] goes to the second state of each pair (b0 set).
+    int dcnt = 0, didx[4];
+    {
+        uint32_t dq = ~t9 & (t9 >> 1) & 0xFFu;
+        dcnt = __popc(dq);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int q = dq ? __ffs(dq) - 1 : 0;
+            dq &= dq - 1;
+            didx[k] = n - 2 - q;
+        }
+    }
+    const bool t0set = t9 & 1;
     uint32_t it = 0;
     int cslot = 0;
     uint32_t cph = 0;
@@ -282,12 +281,18 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
             V2<X1>::ldg(s + pb0, xb[0], xb[1], once);
             V2<X1>::ldg(s + pb1, xb[2], xb[3], once);
         }
-        // low diagonal prefixes of this system
+        // diagonal below the tile level (reassociated: these stages may)
         G d0, d1, d2, d3;
         {
-            const G *dt = dtab_all + (size_t(sys) * 2 + (top ? 1 : 0)) * kTile;
-            const G *q0 = dt + pb0, *q1 = dt + pb1;
-            d0 = q0[0]; d1 = q0[1]; d2 = q1[0]; d3 = q1[1];
+            G sd = top ? G(0) : r0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < dcnt) sd += batch_rate<G>(rs, didx[k]);
+            const G e0 = t0set ? -(sd + rn1) : -sd;  // first state of a pair (b0 clear)
+            const G e1 = -(sd + rn);                 // second state (b0 set)
+            d0 = e0; d1 = e1;
+            d2 = b9 ? e0 : e0 - r9;
+            d3 = b9 ? e1 : e1 - r9;
         }
         G a0 = G(0), a1 = G(0), a2 = G(0), a3 = G(0);
         int eslot = 0;

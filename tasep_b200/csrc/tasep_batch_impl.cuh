@@ -64,8 +64,6 @@ struct tasep_batch {
     double *X = nullptr;
     void *V[3] = {nullptr, nullptr, nullptr};
     double *rates = nullptr;
-    double *dtab_d = nullptr;
-    float *dtab_f = nullptr;
     double *partials = nullptr;
     unsigned *counters = nullptr;
     BatchExit *ex = nullptr;
@@ -86,10 +84,9 @@ template <typename E> tasep_status batch_enqueue_step_t(tasep_batch *b, const Ba
     BatchParams p = base;
     tasep_status s;
     const double h = base.h;
-    p.g = b->X; p.out = b->V[0]; p.dtab = b->dtab_d; p.hc = 0.0;
+    p.g = b->X; p.out = b->V[0]; p.hc = 0.0;
     if ((s = launch_batch<ST_H1, E>(p, grid, b->stream))) return s;
     p.g = b->V[0]; p.out = b->V[1]; p.hc = h / 4;
-    p.dtab = (sizeof(E) == 4) ? static_cast<const void *>(b->dtab_f) : static_cast<const void *>(b->dtab_d);
     if ((s = launch_batch<ST_H2, E>(p, grid, b->stream))) return s;
     p.g = b->V[1]; p.s0 = b->V[0]; p.out = b->V[2]; p.hc = h / 3;
     if ((s = launch_batch<ST_H3, E>(p, grid, b->stream))) return s;
@@ -369,8 +366,6 @@ tasep_status tasep_batch_create(int n, int nsys, int precision, int device, void
     bool ok = cudaMalloc(&b->X, tot * sizeof(double)) == cudaSuccess;
     for (int i = 0; i < 3 && ok; ++i) ok = cudaMalloc(&b->V[i], tot * sv) == cudaSuccess;
     ok = ok && cudaMalloc(&b->rates, sizeof(double) * nsys * (n + 1)) == cudaSuccess &&
-         cudaMalloc(&b->dtab_d, sizeof(double) * nsys * 2 * kTile) == cudaSuccess &&
-         cudaMalloc(&b->dtab_f, sizeof(float) * nsys * 2 * kTile) == cudaSuccess &&
          cudaMalloc(&b->partials, sizeof(double) * nsys * tps * kConsumerWarps) == cudaSuccess &&
          cudaMalloc(&b->counters, sizeof(unsigned) * nsys) == cudaSuccess &&
          cudaMalloc(&b->ex, sizeof(BatchExit) * nsys) == cudaSuccess &&
@@ -393,8 +388,6 @@ tasep_status tasep_batch_destroy(tasep_batch *b) {
     cudaFree(b->X);
     for (auto &v : b->V) cudaFree(v);
     cudaFree(b->rates);
-    cudaFree(b->dtab_d);
-    cudaFree(b->dtab_f);
     cudaFree(b->partials);
     cudaFree(b->counters);
     cudaFree(b->ex);
@@ -412,11 +405,6 @@ tasep_status tasep_batch_set_rates(tasep_batch *b, const double *rates) {
     if (!b || !rates) return fail(TASEP_ERR_INVALID, "null argument");
     CU_TRY(cudaSetDevice(b->device));
     CU_TRY(cudaMemcpy(b->rates, rates, sizeof(double) * b->nsys * (b->n + 1), cudaMemcpyHostToDevice));
-    batch_setup_kernel<double><<<256, 256, 0, b->stream>>>(b->n, b->nsys, b->rates, b->dtab_d);
-    CU_TRY(cudaGetLastError());
-    batch_setup_kernel<float><<<256, 256, 0, b->stream>>>(b->n, b->nsys, b->rates, b->dtab_f);
-    CU_TRY(cudaGetLastError());
-    CU_TRY(cudaStreamSynchronize(b->stream));
     b->rates_set = true;
     return TASEP_OK;
 }
