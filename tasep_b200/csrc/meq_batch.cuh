@@ -41,6 +41,7 @@ struct BatchParams {
     const void *s0, *s1;      // per-state extras (batched)
     void *out;
     double h, hc;
+    double cx;  // RK4 sweeps 2, 3: coefficient of the own gathered value; 4: of v2
     const double *rates;      // [nsys][n+1]
     double *partials;         // [nsys][tiles per system][kConsumerWarps]
     unsigned int *counters;   // [nsys]
@@ -380,12 +381,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
             const G Tv = acc[j];
             if constexpr (S == ST_H1) {
                 o[j] = static_cast<O>(p.h * Tv);
-            } else if constexpr (S == ST_H2) {
-                o[j] = static_cast<O>(xv[j] + static_cast<G>(p.hc) * Tv);
-            } else if constexpr (S == ST_H3) {
-                o[j] = static_cast<O>(xa[j] + static_cast<G>(p.hc) * Tv);
+            } else if constexpr (S == ST_H2 || S == ST_H3) {
+                o[j] = static_cast<O>(static_cast<G>(p.cx) * xv[j] + static_cast<G>(p.hc) * Tv);
             } else {
-                const double D = static_cast<double>(xa[j]) + p.hc * static_cast<double>(Tv);
+                const double D = p.cx * static_cast<double>(xa[j]) + p.hc * static_cast<double>(Tv);
                 o[j] = xb[j] + D;
                 cs += fabs(D);
             }

@@ -31,6 +31,30 @@ struct ExitState {
     double pad;
 };
 
+// Classical RK4 for constant rates.  With z = hM the step is the degree-4
+// Taylor polynomial x' = x + z x + z^2 x/2 + z^3 x/6 + z^4 x/24, i.e.
+// x' = x + z Q(z) x with 24 Q(z) = z^3 + 4 z^2 + 12 z + 24 = (z - r)(z^2 + p z + q),
+// r the real root, p = 4 + r, q = -24/r.  The sweeps evaluate it as
+//   v1 = z x,  v2 = (z - r) v1,  w = (z + p) v2,  x' = x + (z w + q v2) / 24,
+// four generator applications of which only the last reads an operand besides
+// its gathered vector and the state: 80 B per state per step in FP64 (a
+// Horner scheme needs 88: its third sweep also reads z x).  The intermediate
+// vectors stay within a small factor of v1 (|r| < 3, p, q > 0): no cancellation.
+struct Rk4Factors {
+    double r, p, q;
+};
+inline Rk4Factors rk4_factors() {
+    double r = -2.9;  // Newton's method on z^3 + 4 z^2 + 12 z + 24 (one real root near -2.9)
+    for (int i = 0; i < 60; ++i) {
+        const double f = ((r + 4.0) * r + 12.0) * r + 24.0;
+        const double d = (3.0 * r + 8.0) * r + 12.0;
+        const double nr = r - f / d;
+        if (nr == r) break;
+        r = nr;
+    }
+    return {r, 4.0 + r, -24.0 / r};
+}
+
 // Rates for one launch: constant, or the time-variant functions of
 // src/lib/matvec.c:44-68 evaluated at the stage time.
 struct RateSpec {
@@ -107,19 +131,36 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 // |r| |z - 1/6| < 12 ulp(v) 2^-56, while for a 53-bit s = S 2^E the distance
 // from S 2^E / 6 to any midpoint of its binade is |8S - 3(2k+1)| 2^E / 48 or
 // |4S - 3(2k+1)| 2^E / 24, an odd multiple of at least 2^E / 48 >= ulp(v) / 12.
-// The argument needs s, q and r normal: 2^-900 <= |s| <= 2^1000.  Zeros (most
-// states early in a run from a pure state) are their own quotient; the rest
-// (subnormals, infinities, NaN) take the IEEE division.
-__device__ __forceinline__ double div6_rn(double s) {
+// The argument needs s, q and r normal: 2^-900 <= |s| <= 2^1000.  +0 (most
+// states early in a run from a pure state) also comes out exact; the rest
+// (-0, subnormals, infinities, NaN) take the IEEE division.
+__device__ __forceinline__ double div6_fast(double s) {
     constexpr double z = 1.0 / 6.0;  // RN(1/6), folded by the compiler
+    const double q = __dmul_rn(s, z);
+    const double r = __fma_rn(-q, 6.0, s);
+    return __fma_rn(r, z, q);
+}
+// s for which div6_fast is the IEEE quotient: the normal range above and +0
+// (q = r = +0); -0 would come out as +0.
+__device__ __forceinline__ bool div6_fast_ok(double s) {
     const double a = fabs(s);
-    if (a >= 0x1p-900 && a <= 0x1p+1000) {
-        const double q = __dmul_rn(s, z);
-        const double r = __fma_rn(-q, 6.0, s);
-        return __fma_rn(r, z, q);
-    }
-    if (a == 0.0) return s;
+    return (a >= 0x1p-900 && a <= 0x1p+1000) || __double_as_longlong(s) == 0;
+}
+__device__ __forceinline__ double div6_rn(double s) {
+    if (div6_fast_ok(s)) return div6_fast(s);
     return __ddiv_rn(s, 6.0);
+}
+// Four quotients per thread with one warp vote: the branch-free fast path
+// unless some value in the warp needs the division.
+__device__ __forceinline__ void div6_rn4(const double (&s)[4], double (&d)[4]) {
+    const bool ok = div6_fast_ok(s[0]) && div6_fast_ok(s[1]) && div6_fast_ok(s[2]) && div6_fast_ok(s[3]);
+    if (__all_sync(__activemask(), ok)) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) d[j] = div6_fast(s[j]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) d[j] = div6_rn(s[j]);
+    }
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {

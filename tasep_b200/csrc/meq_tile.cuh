@@ -68,6 +68,7 @@ struct TileParams {
     const void *s0, *s1, *s2;  // per-state extra inputs
     void *out;
     double h, hc;              // step and stage coefficient
+    double cx;                 // RK4 sweeps 2, 3: coefficient of the own gathered value; 4: of v2
     double t;                  // stage time
     double *partials;          // per-CTA L1 partial sums (final stages)
     unsigned int *counter;     // last-CTA ticket
@@ -105,7 +106,7 @@ template <typename E> struct StageT<ST_H2, E> {
 };
 template <typename E> struct StageT<ST_H3, E> {
     using G = E; using O = E; using X0 = E; using X1 = E; using X2 = E;
-    static constexpr int NX = 1; static constexpr bool FINAL = false; static constexpr bool EXACT = false;
+    static constexpr int NX = 0; static constexpr bool FINAL = false; static constexpr bool EXACT = false;
 };
 template <typename E> struct StageT<ST_H4, E> {
     using G = E; using O = double; using X0 = E; using X1 = double; using X2 = double;
@@ -525,6 +526,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         const G acc[4] = {a0, a1, a2, a3};
         const G xv[4] = {x0, x1, x2, x3};
         O o[4];
+        double s6[4];  // REF, U4: (k1 + 2 k2 + 2 k3 + k4), to be divided by 6
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const G Tv = acc[j];
@@ -533,17 +535,13 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
             } else if constexpr (S == ST_REF) {
                 const double kv = __dmul_rn(p.h, Tv);
                 const double k2 = __dmul_rn(2.0, kv);
-                const double D = div6_rn(__dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv));
-                o[j] = __dadd_rn(xv[j], D);
-                cs += fabs(D);
+                s6[j] = __dadd_rn(__dadd_rn(__dadd_rn(kv, k2), k2), kv);
             } else if constexpr (S == ST_H1) {
                 o[j] = static_cast<O>(p.h * Tv);
-            } else if constexpr (S == ST_H2) {
-                o[j] = static_cast<O>(xv[j] + static_cast<G>(p.hc) * Tv);
-            } else if constexpr (S == ST_H3) {
-                o[j] = static_cast<O>(xa[j] + static_cast<G>(p.hc) * Tv);
-            } else if constexpr (S == ST_H4) {
-                const double D = static_cast<double>(xa[j]) + p.hc * static_cast<double>(Tv);
+            } else if constexpr (S == ST_H2 || S == ST_H3) {  // v2 = (z - r) v1, w = (z + p) v2
+                o[j] = static_cast<O>(static_cast<G>(p.cx) * xv[j] + static_cast<G>(p.hc) * Tv);
+            } else if constexpr (S == ST_H4) {  // x' = x + (z w + q v2) / 24
+                const double D = p.cx * static_cast<double>(xa[j]) + p.hc * static_cast<double>(Tv);
                 o[j] = xb[j] + D;
                 cs += fabs(D);
             } else if constexpr (S == ST_U1) {
@@ -556,9 +554,16 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
                 const double k2 = 2.0 * (xc[j] - x);
                 const double k3 = xv[j] - x;
                 const double k4 = __dmul_rn(p.h, Tv);
-                const double D = div6_rn(__dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4));
-                o[j] = __dadd_rn(x, D);
-                cs += fabs(D);
+                s6[j] = __dadd_rn(__dadd_rn(__dadd_rn(k1, 2.0 * k2), 2.0 * k3), k4);
+            }
+        }
+        if constexpr (S == ST_REF || S == ST_U4) {
+            double D[4];
+            div6_rn4(s6, D);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                o[j] = __dadd_rn(S == ST_REF ? double(xv[j]) : double(xa[j]), D[j]);
+                cs += fabs(D[j]);
             }
         }
         V2<O>::stg(out + gT + pb0, o[0], o[1], once);

@@ -246,14 +246,17 @@ tasep_status enqueue_step_t(tasep_meq *m, unsigned long long step, double t, dou
         p.t = t + h; p.g = m->V[2]; p.s0 = X; p.s1 = m->V[0]; p.s2 = m->V[1]; p.out = X;
         return run_stage<ST_U4, double>(m, p);
     }
+    // classical RK4 in factored form (Rk4Factors): v1 = z x, v2 = (z - r) v1,
+    // w = (z + p) v2, x' = x + (z w + q v2) / 24
+    static const Rk4Factors F = rk4_factors();
     p.t = t;
     p.g = X; p.out = m->V[0];
     if ((s = run_stage<ST_H1, E>(m, p))) return s;
-    p.g = m->V[0]; p.out = m->V[1]; p.hc = h / 4;
+    p.g = m->V[0]; p.out = m->V[1]; p.hc = h; p.cx = -F.r;
     if ((s = run_stage<ST_H2, E>(m, p))) return s;
-    p.g = m->V[1]; p.s0 = m->V[0]; p.out = m->V[2]; p.hc = h / 3;
+    p.g = m->V[1]; p.out = m->V[2]; p.hc = h; p.cx = F.p;
     if ((s = run_stage<ST_H3, E>(m, p))) return s;
-    p.g = m->V[2]; p.s0 = m->V[0]; p.s1 = X; p.out = X; p.hc = h / 2;
+    p.g = m->V[2]; p.s0 = m->V[1]; p.s1 = X; p.out = X; p.hc = h / 24; p.cx = F.q / 24;
     return run_stage<ST_H4, E>(m, p);
 }
 

@@ -84,13 +84,15 @@ template <typename E> tasep_status batch_enqueue_step_t(tasep_batch *b, const Ba
     BatchParams p = base;
     tasep_status s;
     const double h = base.h;
+    // classical RK4 in factored form, as the single-system sweep (Rk4Factors)
+    static const Rk4Factors F = rk4_factors();
     p.g = b->X; p.out = b->V[0]; p.hc = 0.0;
     if ((s = launch_batch<ST_H1, E>(p, grid, b->stream))) return s;
-    p.g = b->V[0]; p.out = b->V[1]; p.hc = h / 4;
+    p.g = b->V[0]; p.out = b->V[1]; p.hc = h; p.cx = -F.r;
     if ((s = launch_batch<ST_H2, E>(p, grid, b->stream))) return s;
-    p.g = b->V[1]; p.s0 = b->V[0]; p.out = b->V[2]; p.hc = h / 3;
+    p.g = b->V[1]; p.out = b->V[2]; p.hc = h; p.cx = F.p;
     if ((s = launch_batch<ST_H3, E>(p, grid, b->stream))) return s;
-    p.g = b->V[2]; p.s0 = b->V[0]; p.s1 = b->X; p.out = b->X; p.hc = h / 2;
+    p.g = b->V[2]; p.s0 = b->V[1]; p.s1 = b->X; p.out = b->X; p.hc = h / 24; p.cx = F.q / 24;
     if ((s = launch_batch<ST_H4, E>(p, grid, b->stream))) return s;
     // systems that converged in this step leave the running list
     batch_compact_kernel<<<1, 1024, 0, b->stream>>>(b->ex, b->nsys, b->list, b->count);
