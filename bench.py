@@ -45,13 +45,15 @@ UNIT = "steps/s"
 
 # algorithmic bytes per state of each kernel: the vectors it must read and write once
 ALG_BYTES = {
-    ("meq_ref_step", 0): 16, ("meq_rk4_h1", 0): 16, ("meq_rk4_h2", 0): 16, ("meq_rk4_h3", 0): 24,
-    ("meq_rk4_h4", 0): 32, ("meq_rk4_h1", 1): 12, ("meq_rk4_h2", 1): 8, ("meq_rk4_h3", 1): 12,
+    # constant-rate RK4 in factored form: v1 = z x, v2 = (z - r) v1, w = (z + p) v2,
+    # x' = x + (z w + q v2) / 24 (each sweep reads its gathered vector once)
+    ("meq_ref_step", 0): 16, ("meq_rk4_h1", 0): 16, ("meq_rk4_h2", 0): 16, ("meq_rk4_h3", 0): 16,
+    ("meq_rk4_h4", 0): 32, ("meq_rk4_h1", 1): 12, ("meq_rk4_h2", 1): 8, ("meq_rk4_h3", 1): 8,
     ("meq_rk4_h4", 1): 24,
     # time-variant RK4: materialised stage inputs (u2, u3, u4), k recovered in the last stage
     ("meq_rk4_u1", 0): 16, ("meq_rk4_u2", 0): 24, ("meq_rk4_u3", 0): 24, ("meq_rk4_u4", 0): 40,
 }
-STEP_BYTES = {(1, 0): 88, (1, 1): 56, (0, 0): 16, (1, 0, "timevar"): 104}
+STEP_BYTES = {(1, 0): 80, (1, 1): 52, (0, 0): 16, (1, 0, "timevar"): 104}
 
 
 def config_rates(n, seed=1):

@@ -194,8 +194,7 @@ tasep_status tasep_meq_profile_read(tasep_meq *m, const char **names, double *ms
 
 /* ---- batched parameter sweeps --------------------------------------------
  * nsys independent systems of the same length n (kTileBits < n <= 24), each
- * with its own n+1 rates, integrated with classical RK4 (Horner form; FP64 or
- * MIXED) until each meets the exit rule on its own.  The reference has no
+ * with its own n+1 rates, integrated with classical RK4 (FP64 or MIXED) until each meets the exit rule on its own.  The reference has no
  * batching; this replaces running bin/masterEquation once per rate vector.
  * Converged systems retire: later steps skip them.  Steps run as replays of a
  * CUDA graph of a few steps; the sweep schedule (tiles interleaved over the

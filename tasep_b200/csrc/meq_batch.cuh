@@ -1,14 +1,14 @@
 // meq_batch.cuh - many independent systems of the same length in one sweep.
 //
 // The batch is one array of nsys * 2^n states; system s owns states
-// [s*2^n, (s+1)*2^n).  A launch applies one classical-RK4 stage (Horner form,
-// see meq_tile.cuh) to every system that has not converged yet: tiles of
+// [s*2^n, (s+1)*2^n).  A launch applies one classical-RK4 sweep (factored
+// form, Rk4Factors) to every system that has not converged yet: tiles of
 // 2^kTileBits states, a producer warp streaming each tile and its partner
 // tiles (partners never leave their system) into shared memory with
 // cp.async.bulk, 16 consumer warps in the pair layout of meq_tile.cuh.  What
 // differs from the single-system kernel:
-//   * rates and the low diagonal prefix table are per system, in global
-//     memory (built once by batch_setup_kernel);
+//   * rates are per system, in global memory; each thread forms the diagonal
+//     of its four states from its fixed low-bit pairs and those rates;
 //   * the L1 norm and the exit rule are per system: each warp stores its
 //     partial sum in a fixed slot, a per-system ticket finds the last warp,
 //     which adds the system's slots in order and updates that system's exit
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
     using O = typename Tr::O;
     using X0 = typename Tr::X0;
     using X1 = typename Tr::X1;
-    static_assert(!Tr::EXACT && Tr::NX <= 2, "batched sweeps run the RK4 (Horner) stages");
+    static_assert(!Tr::EXACT && Tr::NX <= 2, "batched sweeps run the constant-rate RK4 sweeps");
     using LYB = TileLayout<S, E>;
     constexpr int gb = LYB::gb;
     // no diagonal table in shared memory here, so the ring gets that space too

@@ -10,8 +10,10 @@ namespace tasep {
 constexpr int kMaxN = 33;
 constexpr int kMaxR = kMaxN + 1;
 
-// Kernel flavours.  REF is the reference step; H1..H4 the four stages of
-// classical RK4 written as a Horner scheme (constant rates); U1..U4 the four
+// Kernel flavours.  REF is the reference step; H1..H4 the four sweeps of
+// classical RK4 for constant rates (the factored form of Rk4Factors in the
+// tile and batched sweeps, a Horner scheme in the small and cluster-resident
+// kernels); U1..U4 the four
 // stages of classical RK4 with materialised stage inputs (time-variant
 // rates); APPLY is y = M x.
 enum Stage : int {

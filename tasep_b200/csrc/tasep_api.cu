@@ -138,7 +138,7 @@ struct tasep_meq {
     unsigned long long N = 0, ntiles = 0;
     int nsm = 0, grid = 0;
     double *X[2] = {nullptr, nullptr};
-    void *V[3] = {nullptr, nullptr, nullptr};  // A,B,C (Horner) or U2,U3,U4 (time-variant RK4)
+    void *V[3] = {nullptr, nullptr, nullptr};  // v1, v2, w (factored RK4) or U2,U3,U4 (time-variant RK4)
     double *partials = nullptr;
     unsigned *counter = nullptr;
     ExitState *ex = nullptr;

@@ -1,7 +1,9 @@
 """Mixed precision: does a compensated state update matter?  (CPU model.)
 
-The mixed integrator stores the three Horner stage vectors in FP32 and keeps
-the state, the increment D = a + (h/2) M c and the update x + D in FP64.  A
+The mixed integrator stores the three intermediate vectors of the factored
+RK4 step (v1 = z x, v2 = (z - r) v1, w = (z + p) v2 with z = hM) in FP32 and
+keeps the state, the increment D = (z w + q v2) / 24 and the update x + D in
+FP64.  A
 compensated (Kahan) update would also carry the rounding error of x + D from
 step to step, at the price of one more vector (4 B per state: n = 33 would no
 longer fit in one GPU).  This model of the mixed step (FP64 products rounded
@@ -30,11 +32,14 @@ def mixed_model_run(n, r, h, compensated, max_steps=400000, tol=1e-10, stop_coun
     x[0] = 1.0
     comp = np.zeros(1 << n)
     early = 0
+    rr = np.roots([1.0, 4.0, 12.0, 24.0])
+    rt = float(rr[np.argmin(np.abs(rr.imag))].real)  # the real root of 24 Q(z)
+    p, q = 4.0 + rt, -24.0 / rt
     for i in range(max_steps):
-        a = f32(h * O.apply(n, r, x))
-        b = f32(a + (h / 4) * O.apply(n, r, a))
-        c = f32(a + (h / 3) * O.apply(n, r, b))
-        D = a + (h / 2) * O.apply(n, r, c)
+        v1 = f32(h * O.apply(n, r, x))
+        v2 = f32(h * O.apply(n, r, v1) - rt * v1)
+        w = f32(h * O.apply(n, r, v2) + p * v2)
+        D = (h * O.apply(n, r, w) + q * v2) / 24.0
         if compensated:
             y = D - comp
             t = x + y
