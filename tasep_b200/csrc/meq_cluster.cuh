@@ -16,7 +16,7 @@
 // cluster writes it back and takes the next one from a global queue, so
 // converged systems retire without costing the others anything.
 //
-// One RK4 step (constant rates, Horner form as meq_tile.cuh):
+// One RK4 step (constant rates, Horner form; the tile sweeps use the factored form):
 //   H1 a = h M x          (gathers x)
 //   H2 b = a + h/4 M a    (gathers a)
 //   H3 c = a + h/3 M b    (gathers b; c kept in registers until every CTA
