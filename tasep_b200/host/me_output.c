@@ -59,47 +59,65 @@ static void *fmt_worker(void *arg) {
     return NULL;
 }
 
+/* Formats lines [b0, b1) on the threads of one buffer set; returns how many
+ * jobs were started (tids[t] == 0 marks a job run on the calling thread). */
+static int fmt_launch(fmt_job *jobs, pthread_t *tids, int threads, uint64_t per, int n, const double *x,
+                      uint64_t b0, uint64_t b1) {
+    int used = 0;
+    for (int t = 0; t < threads; t++) {
+        uint64_t s = b0 + (uint64_t)t * per, e = s + per;
+        if (s >= b1) break;
+        if (e > b1) e = b1;
+        jobs[t].n = n;
+        jobs[t].x = x;
+        jobs[t].begin = s;
+        jobs[t].end = e;
+        if (pthread_create(&tids[t], NULL, fmt_worker, &jobs[t]) != 0) fmt_worker(&jobs[t]), tids[t] = 0;
+        used++;
+    }
+    return used;
+}
+
+/* The file is written in blocks of 2^20 lines; two buffer sets alternate so
+ * that the threads format block k+1 while block k is being written. */
 int me_write_probs(const char *path, int n, const double *x, int threads) {
     FILE *f = fopen(path, "w");
     if (!f) return -1;
     printf("Writing result vector to file '%s'\n", path);
     if (threads < 1) threads = 1;
-    if (threads > 256) threads = 256;
+    if (threads > 128) threads = 128;
     const uint64_t dim = (uint64_t)1 << n;
     const uint64_t block = (uint64_t)1 << 20;
     const size_t line_max = (size_t)n + 2 + 40;
-    fmt_job jobs[256];
-    pthread_t tids[256];
+    static fmt_job jobs[2][128];
+    pthread_t tids[2][128];
     uint64_t per = (block + threads - 1) / threads;
-    for (int t = 0; t < threads; t++) {
-        jobs[t].buf = (char *)malloc(per * line_max);
-        if (!jobs[t].buf) {
-            fclose(f);
-            return -2;
-        }
-    }
-    for (uint64_t b0 = 0; b0 < dim; b0 += block) {
-        const uint64_t b1 = b0 + block < dim ? b0 + block : dim;
-        int used = 0;
+    int ok = 1;
+    for (int k = 0; k < 2; k++)
         for (int t = 0; t < threads; t++) {
-            uint64_t s = b0 + (uint64_t)t * per, e = s + per;
-            if (s >= b1) break;
-            if (e > b1) e = b1;
-            jobs[t].n = n;
-            jobs[t].x = x;
-            jobs[t].begin = s;
-            jobs[t].end = e;
-            if (pthread_create(&tids[t], NULL, fmt_worker, &jobs[t]) != 0) fmt_worker(&jobs[t]), tids[t] = 0;
-            used++;
+            jobs[k][t].buf = (char *)malloc(per * line_max);
+            if (!jobs[k][t].buf) ok = 0;
         }
-        for (int t = 0; t < used; t++) {
-            if (tids[t]) pthread_join(tids[t], NULL);
-            fwrite(jobs[t].buf, 1, jobs[t].len, f);
-        }
+    if (!ok) {
+        for (int k = 0; k < 2; k++)
+            for (int t = 0; t < threads; t++) free(jobs[k][t].buf);
+        fclose(f);
+        return -2;
+    }
+    int used[2] = {0, 0};
+    used[0] = fmt_launch(jobs[0], tids[0], threads, per, n, x, 0, dim < block ? dim : block);
+    for (uint64_t b0 = 0, k = 0; b0 < dim; b0 += block, k ^= 1) {
+        const uint64_t b1 = b0 + block < dim ? b0 + block : dim;
+        for (int t = 0; t < used[k]; t++)
+            if (tids[k][t]) pthread_join(tids[k][t], NULL);
+        if (b1 < dim) used[k ^ 1] = fmt_launch(jobs[k ^ 1], tids[k ^ 1], threads, per, n, x, b1,
+                                                b1 + block < dim ? b1 + block : dim);
+        for (int t = 0; t < used[k]; t++) fwrite(jobs[k][t].buf, 1, jobs[k][t].len, f);
         printf("-->%f%%\r", 100. * (double)b1 / (double)dim);
     }
     printf("\n");
-    for (int t = 0; t < threads; t++) free(jobs[t].buf);
+    for (int k = 0; k < 2; k++)
+        for (int t = 0; t < threads; t++) free(jobs[k][t].buf);
     fclose(f);
     return 0;
 }
