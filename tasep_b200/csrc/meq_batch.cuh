@@ -63,6 +63,8 @@ __global__ void batch_compact_kernel(const BatchExit *ex, int nsys, int *list, i
     __shared__ int wtot[32];
     __shared__ int base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    grid_dep_launch();
+    grid_dep_wait();  // the exit flags of the step's last sweep
     if (tid == 0) base = 0;
     __syncthreads();
     for (int s0 = 0; s0 < nsys; s0 += blockDim.x) {
@@ -131,8 +133,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
     const uint32_t tps = 1u << ntb;
     const uint32_t ntiles = uint32_t(p.nsys) << ntb;
     const int R = n + 1;
-    const int na = *p.count;  // running systems this step (set before the launch)
-
+    grid_dep_launch();
     if (tid == 0) {
         c.err = 0;
         for (int b = 0; b < 2; ++b) {
@@ -145,6 +146,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
         }
         fence_mbar_init();
     }
+    // up to here only parameters and shared memory: the previous launch may
+    // still be running
+    grid_dep_wait();
+    const int na = *p.count;  // running systems this step (set before the launch)
     __syncthreads();
     volatile int *errf = &c.err;
     const uint32_t lowmask = ntb >= 2 ? ((1u << (ntb - 1)) - 1) : 0u;

@@ -4,6 +4,7 @@
 
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <utility>
 
 namespace tasep {
 
@@ -163,6 +164,34 @@ __device__ __forceinline__ void div6_rn4(const double (&s)[4], double (&d)[4]) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) d[j] = div6_rn(s[j]);
     }
+}
+
+// Programmatic dependent launch (sweeps launched with the programmatic
+// stream-serialization attribute): grid_dep_launch lets the next sweep's CTAs
+// be scheduled, onto SMs this grid has left, while this grid finishes;
+// grid_dep_wait blocks until the previous grid has completed and its memory
+// is visible.  Nothing before the wait may touch device memory that the
+// previous grid writes or reads.  Both are no-ops for a normal launch.
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// Host side: launch with programmatic stream serialization, so that the
+// kernel's CTAs may start (and run up to grid_dep_wait) while the previous
+// kernel on the stream finishes.  Also valid inside stream capture.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {

@@ -206,8 +206,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
     // and bit scans cost half the integer instructions of 64-bit ones
     const uint32_t ntiles = uint32_t(p.ntiles);
 
+    grid_dep_launch();
     if (tid == 0) {
-        c.skip = (p.skip_if_done && p.ex) ? *reinterpret_cast<volatile int *>(&p.ex->done) : 0;
         c.err = 0;
         for (int b = 0; b < 2; ++b) {
             mbar_init(&c.full[b], 1);
@@ -224,6 +224,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_tile_kernel(const __grid_
         c.rates_d[tid] = r;
         c.rates_f[tid] = static_cast<float>(r);
     }
+    // up to here only parameters and shared memory: the previous sweep may
+    // still be running
+    grid_dep_wait();
+    if (tid == 0) c.skip = (p.skip_if_done && p.ex) ? *reinterpret_cast<volatile int *>(&p.ex->done) : 0;
     __syncthreads();
     if (c.skip) return;
     volatile int *errf = &c.err;

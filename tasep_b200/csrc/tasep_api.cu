@@ -83,8 +83,7 @@ template <int S, typename E, bool kTuned> tasep_status launch_tile_t(const TileP
         CU_TRY(cudaFuncSetAttribute(meq_tile_kernel<S, E, kTuned>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         configured[dev & 63].store(true, std::memory_order_release);
     }
-    meq_tile_kernel<S, E, kTuned><<<grid, kTileThreads, bytes, st>>>(p);
-    CU_TRY(cudaGetLastError());
+    CU_TRY(launch_pdl(meq_tile_kernel<S, E, kTuned>, dim3(grid), dim3(kTileThreads), size_t(bytes), st, p));
     return TASEP_OK;
 }
 

@@ -49,8 +49,7 @@ template <typename E> tasep_status configure_batch_all() {
 }
 
 template <int S, typename E> tasep_status launch_batch(const BatchParams &p, int grid, cudaStream_t st) {
-    meq_batch_kernel<S, E><<<grid, kTileThreads, batch_smem_bytes<S, E>(), st>>>(p);
-    CU_TRY(cudaGetLastError());
+    CU_TRY(launch_pdl(meq_batch_kernel<S, E>, dim3(grid), dim3(kTileThreads), size_t(batch_smem_bytes<S, E>()), st, p));
     return TASEP_OK;
 }
 
@@ -95,7 +94,7 @@ template <typename E> tasep_status batch_enqueue_step_t(tasep_batch *b, const Ba
     p.g = b->V[2]; p.s0 = b->V[1]; p.s1 = b->X; p.out = b->X; p.hc = h / 24; p.cx = F.q / 24;
     if ((s = launch_batch<ST_H4, E>(p, grid, b->stream))) return s;
     // systems that converged in this step leave the running list
-    batch_compact_kernel<<<1, 1024, 0, b->stream>>>(b->ex, b->nsys, b->list, b->count);
+    CU_TRY(launch_pdl(batch_compact_kernel, dim3(1), dim3(1024), 0, b->stream, b->ex, b->nsys, b->list, b->count));
     CU_TRY(cudaGetLastError());
     return TASEP_OK;
 }
@@ -476,7 +475,7 @@ tasep_status tasep_batch_run(tasep_batch *b, const tasep_run_config *rc, int sch
     CU_TRY(cudaMemsetAsync(b->error, 0, sizeof(int), b->stream));
     b->active_host[0] = b->nsys;
     CU_TRY(cudaMemcpyAsync(b->active, b->active_host, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-    batch_compact_kernel<<<1, 1024, 0, b->stream>>>(b->ex, b->nsys, b->list, b->count);
+    CU_TRY(launch_pdl(batch_compact_kernel, dim3(1), dim3(1024), 0, b->stream, b->ex, b->nsys, b->list, b->count));
     CU_TRY(cudaGetLastError());
     cudaEvent_t e0, e1;
     CU_TRY(cudaEventCreate(&e0));
