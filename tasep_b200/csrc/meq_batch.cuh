@@ -7,8 +7,10 @@
 // tiles (partners never leave their system) into shared memory with
 // cp.async.bulk, 16 consumer warps in the pair layout of meq_tile.cuh.  What
 // differs from the single-system kernel:
-//   * rates are per system, in global memory; each thread forms the diagonal
-//     of its four states from its fixed low-bit pairs and those rates;
+//   * rates are per system: each consumer warp copies its system's rates into
+//     a shared-memory row when its next tile belongs to another system, and
+//     each thread forms the diagonal of its four states from its fixed
+//     low-bit pairs and those rates;
 //   * the L1 norm and the exit rule are per system: each warp stores its
 //     partial sum in a fixed slot, a per-system ticket finds the last warp,
 //     which adds the system's slots in order and updates that system's exit
@@ -103,6 +105,8 @@ __device__ __forceinline__ uint32_t batch_tile(const BatchParams &p, uint32_t k,
     return (uint32_t(p.list[e]) << ntb) | t;
 }
 
+constexpr int kWarpRates = 32;  // per-warp row of one system's rates (n + 1 <= 25)
+
 template <typename G> __device__ __forceinline__ G batch_rate(const double *r, int i) {
     return static_cast<G>(__ldg(r + i));
 }
@@ -117,8 +121,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
     static_assert(!Tr::EXACT && Tr::NX <= 2, "batched sweeps run the constant-rate RK4 sweeps");
     using LYB = TileLayout<S, E>;
     constexpr int gb = LYB::gb;
-    // no diagonal table in shared memory here, so the ring gets that space too
-    constexpr int RS0 = (kSmemMax - kCtrlBytes - 2 * gb) / gb;
+    // no diagonal table in shared memory here; each consumer warp keeps the
+    // rates of the system it works on in a row of its own (kWarpRates)
+    constexpr int RS0 = (kSmemMax - kCtrlBytes - 2 * gb - kConsumerWarps * kWarpRates * int(sizeof(G))) / gb;
     constexpr int RS = RS0 < kMaxRing ? RS0 : kMaxRing;
 
     extern __shared__ __align__(128) unsigned char batch_smem[];
@@ -260,6 +265,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
     int cslot = 0;
     uint32_t cph = 0;
     bool ok = true;
+    G *wr = reinterpret_cast<G *>(ring_base + RS * gb) + warp * kWarpRates;  // this warp's rates row
+    uint32_t cur_sys = 0xffffffffu;
 
     for (uint32_t k = 0;; ++k) {
         const uint32_t T = batch_tile(p, k, ntb, ntiles, na);
@@ -271,9 +278,14 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
         const uint32_t hmask = t & ~(t >> 1) & lowmask;
         const uint32_t dhmask = ~t & (t >> 1) & lowmask;
         const unsigned long long gT = (unsigned long long)T * kTile;
-        const double *rs = p.rates + size_t(sys) * R;
-        const G rn = batch_rate<G>(rs, n), r0 = batch_rate<G>(rs, 0), rn1 = batch_rate<G>(rs, n - 1);
-        const G r9 = batch_rate<G>(rs, n - 10), rnL = batch_rate<G>(rs, n - kTileBits);
+        if (sys != cur_sys) {  // warp-uniform: one coalesced load of the system's rates
+            __syncwarp();
+            if (lane < R) wr[lane] = batch_rate<G>(p.rates + size_t(sys) * R, lane);
+            __syncwarp();
+            cur_sys = sys;
+        }
+        const G rn = wr[n], r0 = wr[0], rn1 = wr[n - 1];
+        const G r9 = wr[n - 10], rnL = wr[n - kTileBits];
 
         X0 xa[4];
         X1 xb[4];
@@ -293,7 +305,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
             G sd = top ? G(0) : r0;
 #pragma unroll
             for (int k = 0; k < 4; ++k)
-                if (k < dcnt) sd += batch_rate<G>(rs, didx[k]);
+                if (k < dcnt) sd += wr[didx[k]];
             const G e0 = t0set ? -(sd + rn1) : -sd;  // first state of a pair (b0 clear)
             const G e1 = -(sd + rn);                 // second state (b0 set)
             d0 = e0; d1 = e1;
@@ -321,7 +333,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
         {
             G ds = G(0);
             for (uint32_t mh = dhmask; mh; mh &= mh - 1)
-                ds += batch_rate<G>(rs, n - 1 - kTileBits - (__ffs(mh) - 1));
+                ds += wr[n - 1 - kTileBits - (__ffs(mh) - 1)];
             d0 -= ds; d1 -= ds; d2 -= ds; d3 -= ds;
         }
         a0 = fma(d0, x0, a0); a1 = fma(d1, x1, a1); a2 = fma(d2, x2, a2); a3 = fma(d3, x3, a3);
@@ -339,7 +351,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             if (k < qcnt) {
-                const G rq = batch_rate<G>(rs, qidx[k]);
+                const G rq = wr[qidx[k]];
                 G p0, p1, p2, p3;
                 V2<G>::lds(xs + pb0 + qoff[k], p0, p1);
                 V2<G>::lds(xs + pb1 + qoff[k], p2, p3);
@@ -367,7 +379,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
         for (uint32_t mh = hmask; mh; mh &= mh - 1) {
             if (!mbar_wait(&c.rfull[cslot], cph, errf)) { ok = false; break; }
             const G *pp = reinterpret_cast<const G *>(ring_base + cslot * gb);
-            const G rr = batch_rate<G>(rs, n - 1 - kTileBits - (__ffs(mh) - 1));
+            const G rr = wr[n - 1 - kTileBits - (__ffs(mh) - 1)];
             G p0, p1, p2, p3;
             V2<G>::lds(pp + pb0, p0, p1);
             V2<G>::lds(pp + pb1, p2, p3);
@@ -445,10 +457,12 @@ __global__ void __launch_bounds__(kTileThreads, 1) meq_batch_kernel(const __grid
 }
 
 template <int S, typename E> constexpr int batch_smem_bytes() {
+    using G = typename StageT<S, E>::G;
     constexpr int gb = TileLayout<S, E>::gb;
-    constexpr int RS0 = (kSmemMax - kCtrlBytes - 2 * gb) / gb;
+    constexpr int wr = kConsumerWarps * kWarpRates * int(sizeof(G));
+    constexpr int RS0 = (kSmemMax - kCtrlBytes - 2 * gb - wr) / gb;
     constexpr int RS = RS0 < kMaxRing ? RS0 : kMaxRing;
-    return kCtrlBytes + 2 * gb + RS * gb;
+    return kCtrlBytes + 2 * gb + RS * gb + wr;
 }
 
 }  // namespace tasep
