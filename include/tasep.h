@@ -252,6 +252,15 @@ tasep_status tasep_mlp_loss_grad(tasep_mlp *m, const float *x, const float *t, i
 tasep_status tasep_mlp_train(tasep_mlp *m, const float *x, const float *t, int n, const float *out_weights,
                              int epochs, int batch, float lr, uint64_t seed, float *loss_per_epoch);
 tasep_status tasep_mlp_predict(tasep_mlp *m, const float *x, int n, float *y);
+/* The network's mean-field input feature, on the host: for each of `count`
+ * rate vectors (n+1 doubles each, consecutive), explicit Euler on
+ * d rho_i/dt = J_i - J_(i+1) (J_0 = alpha (1 - rho_0), J_i = r_i rho_(i-1)
+ * (1 - rho_i), J_n = beta rho_(n-1)) from rho = 1/2 with dt = 1/(4 max rate)
+ * for `steps` steps, then clipped to [1e-6, 1 - 1e-6]; rho gets count*n
+ * doubles in site order.  Every operation is the one the Python driver's
+ * numpy form performs, in the same order, so the results are equal bit for
+ * bit.  Needs no device. */
+tasep_status tasep_mean_field_profile(int n, int count, int steps, const double *rates, double *rho);
 /* Initial state P(tau) = P(tau_0) prod_j P(tau_(j+1)|tau_j) from densities
  * rho[j] (site order, n values) and nearest-neighbour covariances cov[j] =
  * <tau_j tau_(j+1)> - rho_j rho_(j+1) (n-1 values).  Covariances are clipped to

@@ -39,7 +39,7 @@ EXPORTS = (
     "tasep_mlp_create", "tasep_mlp_destroy", "tasep_mlp_set_params", "tasep_mlp_get_params", "tasep_mlp_loss_grad",
     "tasep_mlp_train", "tasep_mlp_predict", "tasep_meq_init_pair_markov", "tasep_meq_run_snapshots",
     "tasep_meq_set_cache_policy", "tasep_meq_get_cache_policy", "tasep_test_inject_wait_expiry",
-    "tasep_batch_last_config", "tasep_meq_run_stream", "tasep_test_div6",
+    "tasep_batch_last_config", "tasep_meq_run_stream", "tasep_test_div6", "tasep_mean_field_profile",
 )
 
 

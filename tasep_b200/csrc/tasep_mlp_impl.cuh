@@ -254,6 +254,28 @@ tasep_status tasep_mlp_predict(tasep_mlp *m, const float *x, int n, float *y) {
     return mlp_check(m);
 }
 
+tasep_status tasep_mean_field_profile(int n, int count, int steps, const double *rates, double *rho) {
+    if (n < 1 || n > TASEP_MAX_N || count < 0 || steps < 0 || (count > 0 && (!rates || !rho)))
+        return fail(TASEP_ERR_INVALID, "mean-field profile: n=%d count=%d steps=%d", n, count, steps);
+    double J[TASEP_MAX_N + 1];
+    for (int c = 0; c < count; ++c) {
+        const double *r = rates + size_t(c) * (n + 1);
+        double *x = rho + size_t(c) * n;
+        double rmax = r[0];
+        for (int i = 1; i <= n; ++i) rmax = r[i] > rmax ? r[i] : rmax;
+        const double dt = 0.25 / rmax;
+        for (int i = 0; i < n; ++i) x[i] = 0.5;
+        for (int s = 0; s < steps; ++s) {
+            J[0] = r[0] * (1.0 - x[0]);
+            for (int i = 1; i < n; ++i) J[i] = r[i] * x[i - 1] * (1.0 - x[i]);
+            J[n] = r[n] * x[n - 1];
+            for (int i = 0; i < n; ++i) x[i] += dt * (J[i] - J[i + 1]);
+        }
+        for (int i = 0; i < n; ++i) x[i] = x[i] < 1e-6 ? 1e-6 : (x[i] > 1.0 - 1e-6 ? 1.0 - 1e-6 : x[i]);
+    }
+    return TASEP_OK;
+}
+
 tasep_status tasep_meq_init_pair_markov(tasep_meq *m, const double *rho, const double *cov) {
     if (!valid_handle(m) || !rho || (!cov && m->n > 1)) return fail(TASEP_ERR_INVALID, "null argument");
     const int n = m->n;

@@ -30,12 +30,13 @@ the last site).
 """
 from __future__ import annotations
 
+import ctypes as C
 import os
 import time
 
 import numpy as np
 
-from . import Batch, INIT_EMPTY, INTEGRATOR_RK4, Meq, Mlp, PRECISION_FP64, TasepError, init_pair_markov
+from . import Batch, INIT_EMPTY, INTEGRATOR_RK4, Meq, Mlp, PRECISION_FP64, TasepError, init_pair_markov, lib
 from . import closure
 
 COV_SCALE = 10.0
@@ -59,7 +60,24 @@ def mean_field_profile(rates, steps=MF_STEPS):
     J_i = r_i rho_(i-1) (1 - rho_i), J_n = beta rho_(n-1), from rho = 1/2, with
     dt = 1/(4 max rate) for a fixed number of steps (deterministic; the slow
     modes of long lattices are not fully relaxed, which does not matter for a
-    feature)."""
+    feature).  Computed by tasep_mean_field_profile in the library (the same
+    operations in the same order as _mean_field_profile_numpy, bit for bit,
+    about 100x faster)."""
+    R = np.ascontiguousarray(np.atleast_2d(np.asarray(rates, dtype=np.float64)))
+    c, n1 = R.shape
+    n = n1 - 1
+    rho = np.empty((c, n))
+    L = lib()
+    L.tasep_mean_field_profile.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    st = L.tasep_mean_field_profile(n, c, int(steps), R.ctypes.data_as(C.POINTER(C.c_double)),
+                                    rho.ctypes.data_as(C.POINTER(C.c_double)))
+    if st != 0:
+        raise TasepError(st, L.tasep_last_error().decode())
+    return rho[0] if np.ndim(rates) == 1 else rho
+
+
+def _mean_field_profile_numpy(rates, steps=MF_STEPS):
+    """The same iteration in numpy (the form the network was trained with)."""
     R = np.atleast_2d(np.asarray(rates, dtype=np.float64))
     c, n1 = R.shape
     n = n1 - 1

@@ -119,3 +119,13 @@ def test_pair_field_profile():
     rb, cb = ws.pair_field_profile(R, max_steps=3000)
     r1, c1 = ws.pair_field_profile(R[2], max_steps=3000)
     assert np.allclose(rb[2], r1) and np.allclose(cb[2], c1)
+
+
+def test_mean_field_profile_library_equals_numpy_form():
+    """The library's mean-field feature performs the numpy form's operations in
+    the same order: equal bit for bit, single vectors and batches."""
+    rng = np.random.default_rng(11)
+    for n in (2, 7, 16, 24):
+        R = ws.sample_rates(n, 3, rng)
+        assert np.array_equal(ws.mean_field_profile(R), ws._mean_field_profile_numpy(R))
+        assert np.array_equal(ws.mean_field_profile(R[1]), ws._mean_field_profile_numpy(R[1]))
