@@ -15,18 +15,20 @@
 // tile is 2^kTileBits consecutive states; tile T's index holds the state's
 // bits >= kTileBits.  Per CTA (one per SM, persistent over tiles):
 //   * a producer warp streams, with cp.async.bulk (no multicast), the tile of
-//     g and of each per-state extra input into a double-buffered stage, then
-//     every partner tile this tile needs - the entry tile, the lower half of
-//     tile T+1 (the hop straddling the tile edge) and one tile per active high
-//     hop - into a ring of shared-memory slots;
-//   * 16 consumer warps own one group of 4 consecutive states per thread.
-//     Hops inside a group are register moves; hops between groups read the
-//     staged tile with predicated loads (fully unrolled, so independent chains
-//     interleave); high hops read the ring slots in ascending bit order.  The
-//     diagonal's low part (everything up to bit 9, which precedes the tile-
-//     level terms in the reference's subtraction order) comes from a table
-//     built once per launch, the remaining terms are subtracted in order, so
-//     the reference's rounding sequence is kept exactly.
+//     g into a double-buffered stage, then every partner tile this tile
+//     needs - the entry tile, the lower half of tile T+1 (the hop straddling
+//     the tile edge) and one tile per active high hop - into a ring of
+//     shared-memory slots; per-state extra inputs go straight to registers;
+//   * 16 consumer warps; thread t owns the state pairs {2t, 2t+1} and
+//     {2t+1024, 2t+1025}.  The hop inside a pair is a register move, the one
+//     between neighbouring pairs a shuffle, other in-tile hops read the staged
+//     tile (a per-thread list of partner offsets), high hops read the ring
+//     slots in ascending bit order.  The diagonal's low part (everything up to
+//     bit 9, which precedes the tile-level terms in the reference's
+//     subtraction order) comes from a table built once per launch; the exact
+//     stages subtract the tile-level terms in order, so the reference's
+//     rounding sequence is kept exactly, while the reassociating RK4 sweeps
+//     look their sum up in five-bit window tables.
 // All CTAs sweep the tiles together (natural order, except that the entry bit
 // toggles fastest: sweep_tile), so partner tiles up to a few tens of MB ahead
 // are still in L2 when they are gathered.
